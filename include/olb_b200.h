@@ -1,0 +1,182 @@
+/* openlb_b200 — C ABI of the B200-native collide-and-stream step.
+ *
+ * This is the seam an OpenLB platform specialisation binds to.  In the
+ * reference the same seam is the platform tag: `enum struct Platform`
+ * (src/core/platform/platform.h:35-39), the dispatch switches
+ * (src/core/platform/dispatch.h:40-132) and the per-platform specialisations
+ * of ConcreteBlockLattice (src/core/blockLattice.h:458-701), its population
+ * columns (src/core/platform/gpu/cuda/column.h:100-188) and collision
+ * operators (src/core/platform/gpu/cuda/operator.h:47-126).  Each entry point
+ * below names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Every call returns an olb_b200_status; OLB_B200_OK is 0.  The message of
+ *     the last failure on the calling thread is olb_b200_last_error().  A C++
+ *     host shim turns non-OK into std::runtime_error(olb_b200_last_error()),
+ *     as OpenLB's gpu::cuda::device::check() does (gpu/cuda/device.hh:48-62).
+ *   - Populations cross the ABI in OpenLB's LOGICAL layout: shifted values
+ *     f_i - w_i (src/dynamics/lbm.h:57-63,267-275), structure of arrays
+ *     pops[i*n + cell], cell = (x*ny + y)*nz + z over the core cells (z fastest,
+ *     no overlap/padding; src/core/blockStructure.h:65-75,150), the state after
+ *     the last stream.  The element type is the compute type: double for
+ *     OLB_B200_STORAGE_F64, float otherwise.  How the library keeps them in
+ *     device memory (AA pattern, 16-bit storage) is internal.
+ *   - Host pointers are borrowed for the duration of the call.  Device
+ *     memory, the CUDA stream and any CUDA graphs are owned by the handle.
+ *   - One host thread drives one lattice handle; distinct handles may be used
+ *     from distinct threads.  All device work of a handle is ordered on its
+ *     own non-blocking stream.
+ */
+#ifndef OLB_B200_H
+#define OLB_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OLB_B200_ABI_VERSION 1
+
+typedef struct olb_b200_lattice olb_b200_lattice;
+
+typedef enum {
+  OLB_B200_OK = 0,
+  OLB_B200_ERR_CUDA = 1,        /* a CUDA runtime call failed */
+  OLB_B200_ERR_OOM = 2,         /* device allocation failed */
+  OLB_B200_ERR_ARG = 3,         /* invalid argument */
+  OLB_B200_ERR_DIVERGED = 4,    /* non-finite density/velocity detected */
+  OLB_B200_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+  OLB_B200_ERR_UNSUPPORTED = 6  /* valid request this build cannot serve */
+} olb_b200_status;
+
+typedef enum {
+  OLB_B200_STORAGE_F32 = 0,     /* populations stored as float */
+  OLB_B200_STORAGE_F64 = 1,     /* populations stored and collided in double */
+  OLB_B200_STORAGE_F16 = 2,     /* (f_i - w_i)*2^k_i stored as IEEE half, FP32 math */
+  OLB_B200_STORAGE_BF16 = 3     /* (f_i - w_i)*2^k_i stored as bfloat16, FP32 math */
+} olb_b200_storage;
+
+/* Dynamics kinds; one per reference alias. */
+typedef enum {
+  OLB_B200_DYN_NONE = 0,                 /* NoDynamics              src/dynamics/dynamics.h:51-62 */
+  OLB_B200_DYN_BGK = 1,                  /* BGKdynamics             src/dynamics/dynamics.h:89-98 */
+  OLB_B200_DYN_TRT = 2,                  /* TRTdynamics             src/dynamics/dynamics.h:445-451 */
+  OLB_B200_DYN_SMAGORINSKY = 3,          /* SmagorinskyBGKdynamics  src/dynamics/smagorinskyBGKdynamics.h:37-44 */
+  OLB_B200_DYN_BOUNCE_BACK = 4,          /* BounceBack              src/dynamics/dynamics.h:472-483 */
+  OLB_B200_DYN_BOUNCE_BACK_VELOCITY = 5, /* BounceBackVelocity      src/dynamics/dynamics.h:549-555 */
+  OLB_B200_DYN_FORCED_BGK = 6,           /* ForcedBGKdynamics       src/dynamics/dynamics.h:214 */
+  OLB_B200_DYN_FORCED_TRT = 7            /* ForcedTRTdynamics       src/dynamics/dynamics.h:457-464 */
+} olb_b200_dyn_kind;
+
+typedef struct {
+  int32_t q;            /* 19 (D3Q19) or 27 (D3Q27) */
+  int32_t nx, ny, nz;   /* core extent in cells */
+  int32_t periodic[3];  /* CuboidDecomposition::setPeriodicity */
+  int32_t storage;      /* olb_b200_storage */
+  int32_t device;       /* CUDA device ordinal */
+  int32_t reserved[3];  /* must be 0 */
+} olb_b200_desc;
+
+/* One entry of the per-cell dynamics table.  Parameters mirror the
+ * reference's per-dynamics parameters and fields:
+ *   omega        descriptors::OMEGA             (setParameter<OMEGA>)
+ *   magic        collision::TRT::MAGIC          (src/dynamics/collision.h:210)
+ *   smagorinsky  collision::LES::SMAGORINSKY    (src/dynamics/collisionLES.h:70)
+ *   force        descriptors::FORCE field value (Guo forcing, forcing.h:38-74)
+ *   wall_u       descriptors::VELOCITY field of BounceBackVelocity (defineU)
+ *   wall_rho     FixedDensity RHO field (1 unless defineRho)               */
+typedef struct {
+  int32_t kind;         /* olb_b200_dyn_kind */
+  int32_t reserved;
+  double omega;
+  double magic;
+  double smagorinsky;
+  double force[3];
+  double wall_u[3];
+  double wall_rho;
+} olb_b200_dyn_params;
+
+/* Statistics of one step as OpenLB's LatticeStatistics reports them
+ * (src/core/latticeStatistics.h:49-71, SuperLattice::collectStatistics
+ * src/core/superLattice.hh:61-106), reduced in FP64 on the device. */
+typedef struct {
+  double sum_rho;       /* over cells whose collision reports a statistic */
+  double sum_usqr;
+  double max_usqr;
+  int64_t n_cells;
+  double average_rho;   /* sum_rho / n_cells              (getAverageRho)    */
+  double average_energy;/* 0.5 * sum_usqr / n_cells       (getAverageEnergy) */
+  double max_u;         /* sqrt(max_usqr)                 (getMaxU)          */
+  int64_t n_nonfinite;  /* cells with non-finite rho or |u|^2 */
+} olb_b200_stats;
+
+/* Lifecycle — replaces constructUsingConcretePlatform + ConcreteBlockLattice
+ * ctor (src/core/platform/dispatch.h:106-132, src/core/blockLattice.hh:393-416).
+ * Allocates the population columns; all cells start as NoDynamics with zero
+ * (equilibrium at rest) populations. */
+olb_b200_status olb_b200_create(const olb_b200_desc* desc, olb_b200_lattice** out);
+void olb_b200_destroy(olb_b200_lattice* lattice);
+
+/* Per-cell dynamics — replaces BlockDynamicsMap::set + the per-dynamics masks
+ * and DynamicsPromise (src/core/blockDynamicsMap.h:72-171,266-278) and
+ * setParameter (src/core/blockLattice.h:562-572).  ids[cell] indexes table;
+ * ids == NULL assigns table[0] to every cell.  At most 256 entries; every
+ * fluid entry must use the same collision kind (walls and NoDynamics may be
+ * mixed in freely). */
+olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* lattice, const uint8_t* ids,
+                                      const olb_b200_dyn_params* table, int32_t n_entries);
+
+/* Full population state, host <-> device — replaces
+ * setProcessingContext(Simulation/Evaluation) for POPULATION
+ * (src/core/platform/gpu/cuda/column.hh:157-187,285-296).  Logical layout. */
+olb_b200_status olb_b200_set_populations(olb_b200_lattice* lattice, const void* host_pops);
+olb_b200_status olb_b200_get_populations(olb_b200_lattice* lattice, void* host_pops);
+
+/* The hot path — replaces SuperLattice::collideAndStream
+ * (src/core/superLattice.hh:601-663): collide (gpu/cuda/operator.hh:311-318)
+ * fused with streaming (column.h:144-154, blockLattice.hh:317-339) in one
+ * kernel per step.  Runs `steps` steps.  With stats == NULL the call only
+ * enqueues work on the lattice's stream and returns; with stats != NULL the
+ * last step also reduces the statistics, the call waits for them and returns
+ * OLB_B200_ERR_DIVERGED if any cell was non-finite. */
+olb_b200_status olb_b200_collide_and_stream(olb_b200_lattice* lattice, int32_t steps,
+                                            olb_b200_stats* stats);
+
+/* Density and velocity per cell as SuperLatticeDensity3D / Velocity3D report
+ * them (src/functors/lattice/latticeVelocity3D.hh:65-71,
+ * latticeDensity3D.hh:67), computed on the device: only 4 values per cell
+ * cross PCIe instead of q.  rho: n values, u: 3*n values (component-major).
+ * Element type as for populations. */
+olb_b200_status olb_b200_get_moments(olb_b200_lattice* lattice, void* host_rho, void* host_u);
+
+/* Waits for all work enqueued on the lattice. */
+olb_b200_status olb_b200_synchronize(olb_b200_lattice* lattice);
+
+/* Device time of `steps` collide-and-stream steps, measured with CUDA events
+ * on the lattice's stream (synchronous). */
+olb_b200_status olb_b200_time_steps(olb_b200_lattice* lattice, int32_t steps, float* milliseconds);
+
+/* Introspection: the lattice's cudaStream_t, the number of steps done, the
+ * bytes of device memory the handle holds, and the launch shape in use. */
+olb_b200_status olb_b200_get_stream(olb_b200_lattice* lattice, void** stream);
+olb_b200_status olb_b200_get_info(olb_b200_lattice* lattice, int64_t* steps_done,
+                                  int64_t* device_bytes, int32_t* block_z, int32_t* block_y);
+
+/* Launch shape of the step kernel (threads along z and y, product <= 512,
+ * block_z a multiple of 32).  0,0 selects the built-in default. */
+olb_b200_status olb_b200_set_launch_shape(olb_b200_lattice* lattice, int32_t block_z, int32_t block_y);
+
+/* Thread-local message of the last failed call on this thread ("" if none). */
+const char* olb_b200_last_error(void);
+
+/* ABI version and a build description (compiler, architecture, flags). */
+int32_t olb_b200_abi_version(void);
+const char* olb_b200_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OLB_B200_H */

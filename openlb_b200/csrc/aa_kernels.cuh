@@ -1,0 +1,422 @@
+// Fused collide-and-stream for sm_100a on the in-place AA pattern.
+//
+// Memory layout in HBM: one column per population i, `stride` elements long
+// (the cell count rounded up to 64 elements, so every column starts on a 256 B
+// boundary), cell = (x*ny + y)*nz + z with z fastest — OpenLB's order
+// (src/core/blockStructure.h:65-75) without the overlap layers.  Periodic and
+// non-periodic faces alike wrap per axis; at non-periodic faces the wrapped
+// values only ever reach wall cells, exactly as OpenLB's unspecified padding
+// values only reach its wall cells.
+//
+// AA pattern (one array, in place):
+//   even step t: cell x reads f_i from column i at x, collides, writes f*_i to
+//                column opp(i) at x.
+//   odd step   : cell x reads f_i from column opp(i) at x - c_i, collides,
+//                writes f*_i to column i at x + c_i.
+// After an odd step the array holds the post-stream state in natural order
+// (f_i(x) in column i at x); after an even step f_i(x) sits in column opp(i)
+// at x - c_i.  Every cell reads and writes exactly the same q slots, so no two
+// cells touch the same slot.  This is equivalent to OpenLB's collide followed
+// by the periodic-shift stream (src/core/blockLattice.hh:317-339,
+// src/core/platform/cpu/sisd/column.h:193-204).
+//
+// Full-way bounce-back (collision::Revert) writes f*_i = f_opp(i) to exactly
+// the slot f_opp(i) was read from, so wall cells need no memory access at
+// all; moving walls add their Nguyen-Ladd term in place.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "lbm_device.cuh"
+
+namespace olb_b200 {
+
+struct Geometry {
+  int32_t nx, ny, nz;
+  uint32_t stride;  // column length in elements
+};
+
+// per-block partial of the fused statistics reduction (FP64)
+struct StatPartial {
+  double sum_rho;
+  double sum_usqr;
+  double max_usqr;
+  unsigned long long n_cells;
+  unsigned long long n_nonfinite;
+};
+
+// ---------------------------------------------------------------------------
+// storage element conversions (plain loads: the array is read and written in
+// place by the same kernel, so the read-only data path is not used)
+
+template <class S, class R> struct Store;
+
+template <class R> struct Store<float, R> {
+  template <class L, int I> OLB_DEV static R load(const float* p) { return R(*p); }
+  template <class L, int I> OLB_DEV static void store(float* p, R v) { *p = float(v); }
+};
+template <class R> struct Store<double, R> {
+  template <class L, int I> OLB_DEV static R load(const double* p) { return R(*p); }
+  template <class L, int I> OLB_DEV static void store(double* p, R v) { *p = double(v); }
+};
+template <class R> struct Store<__half, R> {
+  template <class L, int I> OLB_DEV static R load(const __half* p)
+  {
+    constexpr float inv = 1.f / storage_scale<L>(I);
+    return R(__half2float(*p) * inv);
+  }
+  template <class L, int I> OLB_DEV static void store(__half* p, R v)
+  {
+    constexpr float s = storage_scale<L>(I);
+    *p = __float2half_rn(float(v) * s);
+  }
+};
+template <class R> struct Store<__nv_bfloat16, R> {
+  template <class L, int I> OLB_DEV static R load(const __nv_bfloat16* p)
+  {
+    constexpr float inv = 1.f / storage_scale<L>(I);
+    return R(__bfloat162float(*p) * inv);
+  }
+  template <class L, int I> OLB_DEV static void store(__nv_bfloat16* p, R v)
+  {
+    constexpr float s = storage_scale<L>(I);
+    *p = __float2bfloat16_rn(float(v) * s);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// neighbour offsets with per-axis wrap-around
+
+struct Neighbours {
+  uint32_t xo[3], yo[3], zo[3];
+  OLB_DEV Neighbours(const Geometry& g, int x, int y, int z)
+  {
+    const uint32_t sxy = uint32_t(g.ny) * uint32_t(g.nz);
+    xo[0] = uint32_t(x == 0 ? g.nx - 1 : x - 1) * sxy;
+    xo[1] = uint32_t(x) * sxy;
+    xo[2] = uint32_t(x == g.nx - 1 ? 0 : x + 1) * sxy;
+    yo[0] = uint32_t(y == 0 ? g.ny - 1 : y - 1) * uint32_t(g.nz);
+    yo[1] = uint32_t(y) * uint32_t(g.nz);
+    yo[2] = uint32_t(y == g.ny - 1 ? 0 : y + 1) * uint32_t(g.nz);
+    zo[0] = uint32_t(z == 0 ? g.nz - 1 : z - 1);
+    zo[1] = uint32_t(z);
+    zo[2] = uint32_t(z == g.nz - 1 ? 0 : z + 1);
+  }
+  template <int DX, int DY, int DZ>
+  OLB_DEV uint32_t at() const { return xo[DX + 1] + yo[DY + 1] + zo[DZ + 1]; }
+};
+
+// ---------------------------------------------------------------------------
+// block-level FP64 statistics reduction
+
+OLB_DEV void warp_reduce(double& a, double& b, double& m, unsigned long long& n, unsigned long long& nf)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+    m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    n += __shfl_down_sync(0xffffffffu, n, o);
+    nf += __shfl_down_sync(0xffffffffu, nf, o);
+  }
+}
+
+OLB_DEV void block_stats(double a, double b, double m, unsigned long long n, unsigned long long nf,
+                         StatPartial* out)
+{
+  __shared__ StatPartial warp_part[32];
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int nthreads = blockDim.x * blockDim.y;
+  warp_reduce(a, b, m, n, nf);
+  const int lane = tid & 31, warp = tid >> 5;
+  if (lane == 0) {
+    warp_part[warp] = StatPartial{a, b, m, n, nf};
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (nthreads + 31) >> 5;
+    StatPartial p = lane < nw ? warp_part[lane] : StatPartial{0, 0, 0, 0, 0};
+    warp_reduce(p.sum_rho, p.sum_usqr, p.max_usqr, p.n_cells, p.n_nonfinite);
+    if (lane == 0) {
+      const size_t bid = blockIdx.x + size_t(gridDim.x) * (blockIdx.y + size_t(gridDim.y) * blockIdx.z);
+      out[bid] = p;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the step kernel
+
+// Cells per thread (along y, blockDim.y rows apart) and the launch bounds of
+// the step kernel.  All loads of a thread's cells are issued before any of
+// them is collided, so CELLS_PER_THREAD multiplies the bytes each thread keeps
+// in flight — the quantity that bounds this HBM-streaming kernel.
+#ifndef OLB_B200_CELLS_PER_THREAD
+#define OLB_B200_CELLS_PER_THREAD 1
+#endif
+#ifndef OLB_B200_STEP_THREADS
+#define OLB_B200_STEP_THREADS 256
+#endif
+#ifndef OLB_B200_STEP_MIN_BLOCKS
+#define OLB_B200_STEP_MIN_BLOCKS 2
+#endif
+constexpr int kCellsPerThread = OLB_B200_CELLS_PER_THREAD;
+constexpr int kStepThreads = OLB_B200_STEP_THREADS;
+
+template <int Q, class S, class R, int KIND, bool ODD, bool MASKED, bool STATS>
+__global__ void __launch_bounds__(OLB_B200_STEP_THREADS, OLB_B200_STEP_MIN_BLOCKS)
+aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict__ ids,
+               const DynDevice<R>* __restrict__ table, const DynDevice<R> bulk,
+               StatPartial* __restrict__ partials)
+{
+  using L = Lattice<Q>;
+  using ST = Store<S, R>;
+  constexpr int CPT = kCellsPerThread;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
+  const int x = blockIdx.z;
+
+  double s_rho = 0., s_usqr = 0., s_max = 0.;
+  unsigned long long s_n = 0, s_nf = 0;
+
+  R f[CPT][Q];
+  int kind[CPT];
+  bool go[CPT];
+  uint32_t n[CPT];
+  const DynDevice<R>* p[CPT];
+
+  // phase 1: classify the cells and issue all their loads
+  static_for<0, CPT>([&](auto k) {
+    const int y = y0 + k.value * int(blockDim.y);
+    go[k] = z < g.nz && y < g.ny;
+    kind[k] = KIND;
+    p[k] = &bulk;
+    n[k] = 0;
+    if (go[k]) {
+      n[k] = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
+      if constexpr (MASKED) {
+        const DynDevice<R>* e = table + ids[n[k]];
+        kind[k] = __ldg(&e->kind);
+        p[k] = e;
+      }
+      // full-way bounce-back is a no-op on the AA pattern (see file comment)
+      go[k] = kind[k] != K_BOUNCE_BACK;
+    }
+    if (go[k]) {
+      Neighbours nb(g, x, y, z);
+      static_for<0, Q>([&](auto i) {
+        if constexpr (!ODD) {
+          f[k][i] = ST::template load<L, i.value>(pops + size_t(i.value) * g.stride + n[k]);
+        } else {
+          constexpr int o = L::opp(i);
+          const uint32_t src = nb.template at<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>();
+          f[k][i] = ST::template load<L, o>(pops + size_t(o) * g.stride + src);
+        }
+      });
+    }
+  });
+
+  // phase 2: collide and store
+  static_for<0, CPT>([&](auto k) {
+    if (!go[k]) return;
+    const int y = y0 + k.value * int(blockDim.y);
+    R st_rho = R(0), st_usqr = R(0);
+    bool counted = false;
+    if (kind[k] == KIND) {
+      if constexpr (MASKED) {
+        const DynDevice<R>* e = p[k];
+        DynDevice<R> q;
+        q.omega = __ldg(&e->omega);
+        q.omega_minus = __ldg(&e->omega_minus);
+        q.smago_pre = __ldg(&e->smago_pre);
+        q.tau_mol = __ldg(&e->tau_mol);
+        q.force[0] = __ldg(&e->force[0]);
+        q.force[1] = __ldg(&e->force[1]);
+        q.force[2] = __ldg(&e->force[2]);
+        q.force_relax = __ldg(&e->force_relax);
+        collide_bulk<L, KIND>(f[k], q, st_rho, st_usqr);
+      } else {
+        collide_bulk<L, KIND>(f[k], bulk, st_rho, st_usqr);
+      }
+      counted = true;
+    } else if (MASKED && kind[k] == K_BOUNCE_BACK_VELOCITY) {
+      const DynDevice<R>* e = p[k];
+      revert<L>(f[k]);
+      static_for<1, Q>([&](auto i) {
+        f[k][i] += __ldg(&e->wall_term[i][0]);
+        f[k][i] += __ldg(&e->wall_term[i][1]);
+        f[k][i] += __ldg(&e->wall_term[i][2]);
+      });
+      st_rho = __ldg(&e->wall_rho);
+      const R wu[3] = {__ldg(&e->wall_u[0]), __ldg(&e->wall_u[1]), __ldg(&e->wall_u[2])};
+      st_usqr = norm_sqr(wu);
+      counted = true;
+    }
+    // NoDynamics (and anything else): populations pass through unchanged
+    Neighbours nb(g, x, y, z);
+    static_for<0, Q>([&](auto i) {
+      if constexpr (!ODD) {
+        constexpr int o = L::opp(i);
+        ST::template store<L, o>(pops + size_t(o) * g.stride + n[k], f[k][i]);
+      } else {
+        const uint32_t dst = nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>();
+        ST::template store<L, i.value>(pops + size_t(i.value) * g.stride + dst, f[k][i]);
+      }
+    });
+    if constexpr (STATS) {
+      if (counted) {
+        const double r = double(st_rho), u2 = double(st_usqr);
+        if (isfinite(r) && isfinite(u2)) {
+          s_rho += r; s_usqr += u2; s_max = fmax(s_max, u2); s_n += 1;
+        } else {
+          s_nf += 1;
+        }
+      }
+    }
+  });
+  if constexpr (STATS) {
+    block_stats(s_rho, s_usqr, s_max, s_n, s_nf, partials);
+  }
+}
+
+// Deterministic second pass over the per-block partials (one block).
+__global__ void reduce_partials_kernel(const StatPartial* __restrict__ parts, size_t count,
+                                       StatPartial* __restrict__ out);
+
+// ---------------------------------------------------------------------------
+// logical-layout gather / scatter and moments
+
+// Logical population i at cell x: natural column after an even number of
+// steps, else column opp(i) at x - c_i.
+template <int Q, class S, class R, int I>
+OLB_DEV R logical_pop(const S* __restrict__ pops, const Geometry& g, const Neighbours& nb,
+                      uint32_t n, bool shifted)
+{
+  using L = Lattice<Q>;
+  if (!shifted) {
+    return Store<S, R>::template load<L, I>(pops + size_t(I) * g.stride + n);
+  }
+  constexpr int o = L::opp(I);
+  const uint32_t src = nb.template at<-L::c(I, 0), -L::c(I, 1), -L::c(I, 2)>();
+  return Store<S, R>::template load<L, o>(pops + size_t(o) * g.stride + src);
+}
+
+template <int Q, class S, class R>
+__global__ void gather_logical_kernel(const S* __restrict__ pops, const Geometry g, bool shifted,
+                                      R* __restrict__ out, int i_begin, int i_end)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.nz || y >= g.ny) return;
+  const uint32_t n = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
+  const size_t cells = size_t(g.nx) * g.ny * g.nz;
+  Neighbours nb(g, x, y, z);
+  static_for<0, Q>([&](auto i) {
+    if (i.value >= i_begin && i.value < i_end) {
+      out[size_t(i.value - i_begin) * cells + n] = logical_pop<Q, S, R, i.value>(pops, g, nb, n, shifted);
+    }
+  });
+}
+
+// natural-order write of logical populations (resets the AA parity)
+template <int Q, class S, class R>
+__global__ void scatter_natural_kernel(S* __restrict__ pops, const Geometry g,
+                                       const R* __restrict__ in, int i_begin, int i_end)
+{
+  using L = Lattice<Q>;
+  const size_t cells = size_t(g.nx) * g.ny * g.nz;
+  const size_t n = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+  if (n >= cells) return;
+  static_for<0, Q>([&](auto i) {
+    if (i.value >= i_begin && i.value < i_end) {
+      Store<S, R>::template store<L, i.value>(pops + size_t(i.value) * g.stride + n,
+                                              in[size_t(i.value - i_begin) * cells + n]);
+    }
+  });
+}
+
+// Density / velocity as the reference's Density3D / Velocity3D report them
+// (per-dynamics momenta: src/dynamics/momenta/elements.h).
+template <int Q, class S, class R>
+__global__ void moments_kernel(const S* __restrict__ pops, const Geometry g, bool shifted,
+                               const uint8_t* __restrict__ ids, const DynDevice<R>* __restrict__ table,
+                               R* __restrict__ rho_out, R* __restrict__ u_out)
+{
+  using L = Lattice<Q>;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.nz || y >= g.ny) return;
+  const uint32_t n = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
+  const size_t cells = size_t(g.nx) * g.ny * g.nz;
+  const DynDevice<R>* p = table + (ids ? ids[n] : 0);
+  const int kind = p->kind;
+  R rho, u[3];
+  if (kind == K_BGK || kind == K_TRT || kind == K_SMAGORINSKY || kind == K_FORCED_BGK ||
+      kind == K_FORCED_TRT) {
+    Neighbours nb(g, x, y, z);
+    R f[Q];
+    static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, nb, n, shifted); });
+    if (kind == K_FORCED_BGK || kind == K_FORCED_TRT) {
+      const R gg[3] = {p->force[0], p->force[1], p->force[2]};
+      compute_rho_u_forced<L>(f, gg, rho, u);
+    } else {
+      compute_rho_u<L>(f, rho, u);
+    }
+  } else if (kind == K_BOUNCE_BACK) {
+    rho = p->wall_rho; u[0] = u[1] = u[2] = R(0);
+  } else if (kind == K_BOUNCE_BACK_VELOCITY) {
+    rho = p->wall_rho; u[0] = p->wall_u[0]; u[1] = p->wall_u[1]; u[2] = p->wall_u[2];
+  } else {
+    rho = R(1); u[0] = u[1] = u[2] = R(0);
+  }
+  rho_out[n] = rho;
+  u_out[n] = u[0];
+  u_out[cells + n] = u[1];
+  u_out[2 * cells + n] = u[2];
+}
+
+// ---------------------------------------------------------------------------
+// host-side launch entry points (explicitly instantiated per lattice/storage)
+
+struct StepLaunch {
+  void* pops;
+  Geometry g;
+  const uint8_t* ids;      // device, or nullptr
+  const void* table;       // device DynDevice<R>[]
+  const void* bulk;        // host DynDevice<R>
+  StatPartial* partials;   // device, gridDim product entries
+  int block_z, block_y;
+  cudaStream_t stream;
+};
+
+template <int Q, class S, class R>
+cudaError_t launch_step(const StepLaunch& a, int kind, bool odd, bool masked, bool stats);
+
+template <int Q, class S, class R>
+cudaError_t launch_gather(const void* pops, const Geometry& g, bool shifted, void* out, int i_begin,
+                          int i_end, cudaStream_t stream);
+
+template <int Q, class S, class R>
+cudaError_t launch_scatter(void* pops, const Geometry& g, const void* in, int i_begin, int i_end,
+                           cudaStream_t stream);
+
+template <int Q, class S, class R>
+cudaError_t launch_moments(const void* pops, const Geometry& g, bool shifted, const uint8_t* ids,
+                           const void* table, void* rho, void* u, cudaStream_t stream);
+
+inline dim3 step_grid(const Geometry& g, int bz, int by)
+{
+  const int rows = by * kCellsPerThread;
+  return dim3((g.nz + bz - 1) / bz, (g.ny + rows - 1) / rows, g.nx);
+}
+
+// grid of the gather / moments kernels (one cell per thread)
+inline dim3 cell_grid(const Geometry& g, int bz, int by)
+{
+  return dim3((g.nz + bz - 1) / bz, (g.ny + by - 1) / by, g.nx);
+}
+
+} // namespace olb_b200

@@ -1,0 +1,98 @@
+// Host launchers of the step / gather / scatter / moments kernels.  Included
+// by one translation unit per (lattice, storage) pair, which instantiates
+// them explicitly (see OLB_B200_INSTANTIATE) so the kernel variants compile
+// in parallel.
+#pragma once
+
+#include "aa_kernels.cuh"
+
+namespace olb_b200 {
+
+template <int Q, class S, class R, int KIND>
+static cudaError_t launch_step_kind(const StepLaunch& a, bool odd, bool masked, bool stats)
+{
+  const dim3 block(a.block_z, a.block_y);
+  const dim3 grid = step_grid(a.g, a.block_z, a.block_y);
+  S* pops = static_cast<S*>(a.pops);
+  const DynDevice<R>* table = static_cast<const DynDevice<R>*>(a.table);
+  const DynDevice<R>& bulk = *static_cast<const DynDevice<R>*>(a.bulk);
+#define OLB_LAUNCH(O, M, ST)                                                                  \
+  aa_step_kernel<Q, S, R, KIND, O, M, ST><<<grid, block, 0, a.stream>>>(pops, a.g, a.ids, table, \
+                                                                        bulk, a.partials)
+  if (odd) {
+    if (masked) {
+      if (stats) OLB_LAUNCH(true, true, true); else OLB_LAUNCH(true, true, false);
+    } else {
+      if (stats) OLB_LAUNCH(true, false, true); else OLB_LAUNCH(true, false, false);
+    }
+  } else {
+    if (masked) {
+      if (stats) OLB_LAUNCH(false, true, true); else OLB_LAUNCH(false, true, false);
+    } else {
+      if (stats) OLB_LAUNCH(false, false, true); else OLB_LAUNCH(false, false, false);
+    }
+  }
+#undef OLB_LAUNCH
+  return cudaGetLastError();
+}
+
+template <int Q, class S, class R>
+cudaError_t launch_step(const StepLaunch& a, int kind, bool odd, bool masked, bool stats)
+{
+  switch (kind) {
+  case K_BGK: return launch_step_kind<Q, S, R, K_BGK>(a, odd, masked, stats);
+  case K_TRT: return launch_step_kind<Q, S, R, K_TRT>(a, odd, masked, stats);
+  case K_SMAGORINSKY: return launch_step_kind<Q, S, R, K_SMAGORINSKY>(a, odd, masked, stats);
+  case K_FORCED_BGK: return launch_step_kind<Q, S, R, K_FORCED_BGK>(a, odd, masked, stats);
+  case K_FORCED_TRT: return launch_step_kind<Q, S, R, K_FORCED_TRT>(a, odd, masked, stats);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+template <int Q, class S, class R>
+cudaError_t launch_gather(const void* pops, const Geometry& g, bool shifted, void* out, int i_begin,
+                          int i_end, cudaStream_t stream)
+{
+  const dim3 block(32, 8);
+  const dim3 grid = cell_grid(g, 32, 8);
+  gather_logical_kernel<Q, S, R><<<grid, block, 0, stream>>>(static_cast<const S*>(pops), g, shifted,
+                                                              static_cast<R*>(out), i_begin, i_end);
+  return cudaGetLastError();
+}
+
+template <int Q, class S, class R>
+cudaError_t launch_scatter(void* pops, const Geometry& g, const void* in, int i_begin, int i_end,
+                           cudaStream_t stream)
+{
+  const size_t cells = size_t(g.nx) * g.ny * g.nz;
+  const unsigned threads = 256;
+  const unsigned blocks = unsigned((cells + threads - 1) / threads);
+  scatter_natural_kernel<Q, S, R><<<blocks, threads, 0, stream>>>(static_cast<S*>(pops), g,
+                                                                  static_cast<const R*>(in), i_begin, i_end);
+  return cudaGetLastError();
+}
+
+template <int Q, class S, class R>
+cudaError_t launch_moments(const void* pops, const Geometry& g, bool shifted, const uint8_t* ids,
+                           const void* table, void* rho, void* u, cudaStream_t stream)
+{
+  const dim3 block(32, 8);
+  const dim3 grid = cell_grid(g, 32, 8);
+  moments_kernel<Q, S, R><<<grid, block, 0, stream>>>(static_cast<const S*>(pops), g, shifted, ids,
+                                                       static_cast<const DynDevice<R>*>(table),
+                                                       static_cast<R*>(rho), static_cast<R*>(u));
+  return cudaGetLastError();
+}
+
+} // namespace olb_b200
+
+#define OLB_B200_INSTANTIATE(Q, S, R)                                                              \
+  namespace olb_b200 {                                                                             \
+  template cudaError_t launch_step<Q, S, R>(const StepLaunch&, int, bool, bool, bool);             \
+  template cudaError_t launch_gather<Q, S, R>(const void*, const Geometry&, bool, void*, int, int, \
+                                              cudaStream_t);                                       \
+  template cudaError_t launch_scatter<Q, S, R>(void*, const Geometry&, const void*, int, int,      \
+                                               cudaStream_t);                                      \
+  template cudaError_t launch_moments<Q, S, R>(const void*, const Geometry&, bool, const uint8_t*, \
+                                               const void*, void*, void*, cudaStream_t);           \
+  }

@@ -1,0 +1,365 @@
+// Per-cell lattice-Boltzmann arithmetic for the sm_100a step kernels.
+//
+// Lattice tables follow OpenLB's descriptors bit for bit (direction order and
+// weights: src/descriptor/definition/common.h:120-168 for D3Q19, :313-366 for
+// D3Q27).  The collision functions restate OpenLB's generic templates; the
+// order of the floating-point operations is kept identical to theirs (cited
+// per function) so that a build with -fmad=false reproduces the reference's
+// CPU_SISD results exactly, while the default build lets nvcc contract
+// multiply-adds into FMAs.  Multiplications by a lattice vector component of
+// 0 or +-1 are resolved at compile time (they are exact).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <type_traits>
+#include <utility>
+
+#define OLB_DEV __device__ __forceinline__
+#define OLB_HD __host__ __device__ __forceinline__
+
+namespace olb_b200 {
+
+// ---------------------------------------------------------------------------
+// compile-time iteration
+
+template <int B, int E, class F>
+OLB_HD void static_for(F&& f)
+{
+  if constexpr (B < E) {
+    f(std::integral_constant<int, B>{});
+    static_for<B + 1, E>(static_cast<F&&>(f));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// lattice descriptors
+
+template <int Q> struct Lattice;
+
+template <> struct Lattice<19> {
+  static constexpr int q = 19;
+  static constexpr int half = 9;
+  OLB_HD static constexpr int c(int i, int d)
+  {
+    constexpr int tab[19][3] = {
+      { 0, 0, 0},
+      {-1, 0, 0}, { 0,-1, 0}, { 0, 0,-1}, {-1,-1, 0}, {-1, 1, 0}, {-1, 0,-1},
+      {-1, 0, 1}, { 0,-1,-1}, { 0,-1, 1},
+      { 1, 0, 0}, { 0, 1, 0}, { 0, 0, 1}, { 1, 1, 0}, { 1,-1, 0}, { 1, 0, 1},
+      { 1, 0,-1}, { 0, 1, 1}, { 0, 1,-1}};
+    return tab[i][d];
+  }
+  OLB_HD static constexpr int opp(int i) { return i == 0 ? 0 : (i <= 9 ? i + 9 : i - 9); }
+  OLB_HD static constexpr int wnum(int) { return 1; }
+  OLB_HD static constexpr int wden(int i)
+  {
+    return i == 0 ? 3 : ((i % 9 >= 1 && i % 9 <= 3) ? 18 : 36);
+  }
+};
+
+template <> struct Lattice<27> {
+  static constexpr int q = 27;
+  static constexpr int half = 13;
+  OLB_HD static constexpr int c(int i, int d)
+  {
+    constexpr int tab[27][3] = {
+      { 0, 0, 0},
+      {-1, 0, 0}, { 0,-1, 0}, { 0, 0,-1}, {-1,-1, 0}, {-1, 1, 0}, {-1, 0,-1},
+      {-1, 0, 1}, { 0,-1,-1}, { 0,-1, 1}, {-1,-1,-1}, {-1,-1, 1}, {-1, 1,-1}, {-1, 1, 1},
+      { 1, 0, 0}, { 0, 1, 0}, { 0, 0, 1}, { 1, 1, 0}, { 1,-1, 0}, { 1, 0, 1},
+      { 1, 0,-1}, { 0, 1, 1}, { 0, 1,-1}, { 1, 1, 1}, { 1, 1,-1}, { 1,-1, 1}, { 1,-1,-1}};
+    return tab[i][d];
+  }
+  OLB_HD static constexpr int opp(int i) { return i == 0 ? 0 : (i <= 13 ? i + 13 : i - 13); }
+  OLB_HD static constexpr int wnum(int i)
+  {
+    const int k = i == 0 ? 0 : (i <= 13 ? i : i - 13);
+    return k == 0 ? 8 : (k <= 3 ? 2 : 1);
+  }
+  OLB_HD static constexpr int wden(int i)
+  {
+    const int k = i == 0 ? 0 : (i <= 13 ? i : i - 13);
+    return k == 0 ? 27 : (k <= 3 ? 27 : (k <= 9 ? 54 : 216));
+  }
+};
+
+// Fraction::as<T>() = T(num)/T(den), rounded in T (src/utilities/fraction.h:58-62)
+template <class L, class R>
+OLB_HD constexpr R weight(int i) { return R(L::wnum(i)) / R(L::wden(i)); }
+
+// Power-of-two scale applied to shifted populations in 16-bit storage: the
+// power of two nearest to 1/w_i, so that (f_i - w_i)/w_i-sized deviations use
+// the format's full mantissa.  Exact in binary floating point.
+template <class L>
+OLB_HD constexpr float storage_scale(int i)
+{
+  const int den = L::wden(i), num = L::wnum(i);
+  // nearest power of two to den/num
+  float r = float(den) / float(num);
+  float p = 1.f;
+  while (p * 1.41421356f < r) p *= 2.f;
+  return p;
+}
+
+// ---------------------------------------------------------------------------
+// per-dynamics device parameters (precomputed on the host in R, in the same
+// order the reference evaluates the cell-independent parts)
+
+enum DynKind : int32_t {
+  K_NONE = 0, K_BGK = 1, K_TRT = 2, K_SMAGORINSKY = 3, K_BOUNCE_BACK = 4,
+  K_BOUNCE_BACK_VELOCITY = 5, K_FORCED_BGK = 6, K_FORCED_TRT = 7
+};
+
+template <class R>
+struct DynDevice {
+  int32_t kind;
+  int32_t pad;
+  R omega;          // OMEGA
+  R omega_minus;    // TRT: 1/(magic/(1/omega - 1/2) + 1/2), rounded once (collision.h:239)
+  R smago_pre;      // Smagorinsky prefactor Cs^2 cs^-4 2 sqrt(2)  (collisionLES.h:67-69)
+  R tau_mol;        // 1/omega  (collisionLES.h:71)
+  R force[3];       // FORCE
+  R force_relax;    // 1 - omega/2  (lbm.h:562)
+  R wall_u[3];      // VELOCITY (moving wall)
+  R wall_rho;       // RHO (FixedDensity)
+  R wall_term[27][3]; // 2 rho u_d c_id w_i cs^-2, evaluated as the reference does (collision.h:341-343)
+};
+
+// ---------------------------------------------------------------------------
+// moments
+
+// lbm::computeRho  src/dynamics/lbm.h:266-275
+template <class L, class R>
+OLB_DEV R compute_rho(const R (&f)[L::q])
+{
+  R rho = f[0];
+  static_for<1, L::q>([&](auto i) { rho += f[i]; });
+  rho += R(1);
+  return rho;
+}
+
+// lbm::computeJ  src/dynamics/lbm.h:279-290 (terms with c = 0 add nothing)
+template <class L, class R>
+OLB_DEV void compute_j(const R (&f)[L::q], R (&j)[3])
+{
+  j[0] = R(0); j[1] = R(0); j[2] = R(0);
+  static_for<0, L::q>([&](auto i) {
+    static_for<0, 3>([&](auto d) {
+      constexpr int cc = L::c(i, d);
+      if constexpr (cc == 1) { j[d] += f[i]; }
+      else if constexpr (cc == -1) { j[d] += -f[i]; }
+    });
+  });
+}
+
+// lbm::computeRhoU  src/dynamics/lbm.h:300-307
+template <class L, class R>
+OLB_DEV void compute_rho_u(const R (&f)[L::q], R& rho, R (&u)[3])
+{
+  rho = compute_rho<L>(f);
+  compute_j<L>(f, u);
+  u[0] /= rho; u[1] /= rho; u[2] /= rho;
+}
+
+// ForcedMomentum<BulkMomentum>::computeU after BulkDensity
+// (src/dynamics/momenta/elements.h:1480-1488, :466-475): rho is summed twice
+// in the reference; the second sum is the same value.
+template <class L, class R>
+OLB_DEV void compute_rho_u_forced(const R (&f)[L::q], const R (&g)[3], R& rho, R (&u)[3])
+{
+  compute_rho_u<L>(f, rho, u);
+  u[0] += g[0] * R(0.5); u[1] += g[1] * R(0.5); u[2] += g[2] * R(0.5);
+}
+
+// util::normSqr  src/core/util.h:161-168
+template <class R>
+OLB_DEV R norm_sqr(const R (&u)[3])
+{
+  R s = u[0] * u[0];
+  s += u[1] * u[1];
+  s += u[2] * u[2];
+  return s;
+}
+
+// c_i . u accumulated over d as equilibrium::secondOrder does (lbm.h:53-56)
+template <class L, int I, class R>
+OLB_DEV R c_dot(const R (&u)[3])
+{
+  R cu = R(0);
+  bool first = true;
+  static_for<0, 3>([&](auto d) {
+    constexpr int cc = L::c(I, d);
+    if constexpr (cc != 0) {
+      const R term = cc == 1 ? u[d] : -u[d];
+      if (first) { cu = term; first = false; } else { cu += term; }
+    }
+  });
+  return cu;
+}
+
+// equilibrium::secondOrder  src/dynamics/lbm.h:50-64
+template <class L, int I, class R>
+OLB_DEV R feq2(R rho, const R (&u)[3], R usqr)
+{
+  constexpr R t = weight<L, R>(I);
+  constexpr R inv_cs2 = R(3);
+  const R cu = c_dot<L, I>(u);
+  return rho * t * (R(1) + inv_cs2 * cu + inv_cs2 * inv_cs2 * R(0.5) * cu * cu
+                    - inv_cs2 * R(0.5) * usqr) - t;
+}
+
+// ---------------------------------------------------------------------------
+// collisions (in place on f; return the CellStatistic {rho, uSqr})
+
+// collision::BGK  src/dynamics/collision.h:67-78 with equilibria::SecondOrder
+// (src/dynamics/equilibrium.h:160-167)
+template <class L, class R>
+OLB_DEV void relax_bgk(R (&f)[L::q], R rho, const R (&u)[3], R omega)
+{
+  const R usqr = norm_sqr(u);
+  static_for<0, L::q>([&](auto i) {
+    const R fe = feq2<L, i.value>(rho, u, usqr);
+    f[i] *= R(1) - omega;
+    f[i] += omega * fe;
+  });
+}
+
+// collision::TRT  src/dynamics/collision.h:220-245
+template <class L, class R>
+OLB_DEV void relax_trt(R (&f)[L::q], R rho, const R (&u)[3], R omega, R omega_minus)
+{
+  const R usqr = norm_sqr(u);
+  R fe[L::q];
+  static_for<0, L::q>([&](auto i) { fe[i] = feq2<L, i.value>(rho, u, usqr); });
+  R out[L::q];
+  static_for<0, L::q>([&](auto i) {
+    constexpr int o = L::opp(i);
+    const R fp = R(0.5) * (f[i] + f[o]);
+    const R fm = R(0.5) * (f[i] - f[o]);
+    const R fep = R(0.5) * (fe[i] + fe[o]);
+    const R fem = R(0.5) * (fe[i] - fe[o]);
+    out[i] = f[i] - (omega * (fp - fep) + omega_minus * (fm - fem));
+  });
+  static_for<0, L::q>([&](auto i) { f[i] = out[i]; });
+}
+
+// lbm::addExternalForce (Guo)  src/dynamics/lbm.h:544-566
+template <class L, class R>
+OLB_DEV void add_force(R (&f)[L::q], R rho, const R (&u)[3], R force_relax, const R (&g)[3])
+{
+  constexpr R inv_cs2 = R(3);
+  static_for<0, L::q>([&](auto i) {
+    constexpr R t = weight<L, R>(i);
+    R cu = c_dot<L, i.value>(u);
+    cu *= inv_cs2 * inv_cs2;
+    R term = R(0);
+    static_for<0, 3>([&](auto d) {
+      constexpr int cc = L::c(i, d);
+      term += ((R(cc) - u[d]) * inv_cs2 + cu * R(cc)) * g[d];
+    });
+    term *= t;
+    term *= force_relax;
+    term *= rho;
+    f[i] += term;
+  });
+}
+
+// |Pi_neq|^2 for bulk momenta: lbm::computeStress (lbm.h:310-329) and the
+// norm of ConcreteTuple::computePiNeqNormSqr (momenta/interface.h:163-172),
+// with the reference's double-precision literals kept where they promote.
+template <class L, class R>
+OLB_DEV R pi_neq_norm_sqr(const R (&f)[L::q], R rho, const R (&u)[3])
+{
+  R pi[6];
+  int k = 0;
+  static_for<0, 3>([&](auto a) {
+    static_for<a.value, 3>([&](auto b) {
+      R s = R(0);
+      static_for<0, L::q>([&](auto i) {
+        constexpr int cc = L::c(i, a) * L::c(i, b);
+        if constexpr (cc == 1) { s += f[i]; }
+        else if constexpr (cc == -1) { s += -f[i]; }
+      });
+      s -= rho * u[a] * u[b];
+      if constexpr (a.value == b.value) {
+        s -= R(1) / R(3) * (rho - R(1));
+      }
+      pi[k++] = s;
+    });
+  });
+  R n2 = R(double(pi[0] * pi[0]) + 2. * double(pi[1]) * double(pi[1]) + double(pi[2] * pi[2]));
+  n2 = R(double(n2) + (double(pi[2] * pi[2] + pi[3] * pi[3]) + 2. * double(pi[4]) * double(pi[4])
+                       + double(pi[5] * pi[5])));
+  return n2;
+}
+
+// detail::SmagorinskyEffectiveOmega::computeEffectiveOmega
+// src/dynamics/collisionLES.h:59-80
+template <class L, class R>
+OLB_DEV R smagorinsky_omega(const R (&f)[L::q], R rho, const R (&u)[3], R smago_pre, R tau_mol)
+{
+  const R pnorm = sqrt(pi_neq_norm_sqr<L>(f, rho, u));
+  const R tau_turb = R(0.5) * (sqrt(tau_mol * tau_mol + smago_pre / rho * pnorm) - tau_mol);
+  const R tau_eff = tau_mol + tau_turb;
+  return R(1) / tau_eff;
+}
+
+// collision::Revert  src/dynamics/collision.h:302-309
+template <class L, class R>
+OLB_DEV void revert(R (&f)[L::q])
+{
+  static_for<1, L::half + 1>([&](auto i) {
+    constexpr int o = L::opp(i);
+    const R tmp = f[i];
+    f[i] = f[o];
+    f[o] = tmp;
+  });
+}
+
+// Bulk collision dispatch on the compile-time kind.  Returns the cell
+// statistic (rho, |u|^2) like the reference's collide().
+template <class L, int KIND, class R>
+OLB_DEV void collide_bulk(R (&f)[L::q], const DynDevice<R>& p, R& st_rho, R& st_usqr)
+{
+  R rho, u[3];
+  if constexpr (KIND == K_BGK) {
+    compute_rho_u<L>(f, rho, u);
+    relax_bgk<L>(f, rho, u, p.omega);
+    st_rho = rho; st_usqr = norm_sqr(u);
+  } else if constexpr (KIND == K_TRT) {
+    compute_rho_u<L>(f, rho, u);
+    relax_trt<L>(f, rho, u, p.omega, p.omega_minus);
+    st_rho = rho; st_usqr = norm_sqr(u);
+  } else if constexpr (KIND == K_SMAGORINSKY) {
+    compute_rho_u<L>(f, rho, u);
+    const R w = smagorinsky_omega<L>(f, rho, u, p.smago_pre, p.tau_mol);
+    relax_bgk<L>(f, rho, u, w);
+    st_rho = rho; st_usqr = norm_sqr(u);
+  } else if constexpr (KIND == K_FORCED_BGK || KIND == K_FORCED_TRT) {
+    // forcing::Guo::combined_collision::apply  src/dynamics/forcing.h:53-63
+    const R g[3] = {p.force[0], p.force[1], p.force[2]};
+    compute_rho_u_forced<L>(f, g, rho, u);
+    if constexpr (KIND == K_FORCED_BGK) {
+      relax_bgk<L>(f, rho, u, p.omega);
+    } else {
+      relax_trt<L>(f, rho, u, p.omega, p.omega_minus);
+    }
+    add_force<L>(f, rho, u, p.force_relax, g);
+    st_rho = rho; st_usqr = norm_sqr(u);
+  }
+}
+
+// collision::NguyenLaddCorrection<Revert>  src/dynamics/collision.h:333-346
+template <class L, class R>
+OLB_DEV void collide_moving_wall(R (&f)[L::q], const DynDevice<R>& p)
+{
+  revert<L>(f);
+  static_for<1, L::q>([&](auto i) {
+    f[i] += p.wall_term[i][0];
+    f[i] += p.wall_term[i][1];
+    f[i] += p.wall_term[i][2];
+  });
+}
+
+} // namespace olb_b200

@@ -1,0 +1,616 @@
+// C ABI of the B200-native collide-and-stream (declared in include/olb_b200.h).
+//
+// The handle owns: the population columns (AA layout, one array), the per-cell
+// dynamics ids, the device dynamics table, a staging buffer for logical-layout
+// transfers, the per-block statistics partials and one non-blocking stream.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/olb_b200.h"
+#include "aa_kernels.cuh"
+
+namespace olb_b200 {
+
+// explicit instantiations live in step_q{19,27}_{f32,f64,f16,bf16}.cu
+#define OLB_B200_EXTERN(Q, S, R)                                                                   \
+  extern template cudaError_t launch_step<Q, S, R>(const StepLaunch&, int, bool, bool, bool);      \
+  extern template cudaError_t launch_gather<Q, S, R>(const void*, const Geometry&, bool, void*,    \
+                                                     int, int, cudaStream_t);                      \
+  extern template cudaError_t launch_scatter<Q, S, R>(void*, const Geometry&, const void*, int,    \
+                                                      int, cudaStream_t);                          \
+  extern template cudaError_t launch_moments<Q, S, R>(const void*, const Geometry&, bool,          \
+                                                      const uint8_t*, const void*, void*, void*,   \
+                                                      cudaStream_t);
+OLB_B200_EXTERN(19, float, float)
+OLB_B200_EXTERN(19, double, double)
+OLB_B200_EXTERN(19, __half, float)
+OLB_B200_EXTERN(19, __nv_bfloat16, float)
+OLB_B200_EXTERN(27, float, float)
+OLB_B200_EXTERN(27, double, double)
+OLB_B200_EXTERN(27, __half, float)
+OLB_B200_EXTERN(27, __nv_bfloat16, float)
+
+__global__ void reduce_partials_kernel(const StatPartial* __restrict__ parts, size_t count,
+                                       StatPartial* __restrict__ out)
+{
+  // fixed assignment of partials to threads and a fixed tree: deterministic
+  double a = 0., b = 0., m = 0.;
+  unsigned long long n = 0, nf = 0;
+  for (size_t k = threadIdx.x; k < count; k += blockDim.x) {
+    const StatPartial p = parts[k];
+    a += p.sum_rho;
+    b += p.sum_usqr;
+    m = fmax(m, p.max_usqr);
+    n += p.n_cells;
+    nf += p.n_nonfinite;
+  }
+  __shared__ StatPartial sh[32];
+  warp_reduce(a, b, m, n, nf);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) sh[warp] = StatPartial{a, b, m, n, nf};
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    StatPartial p = lane < nw ? sh[lane] : StatPartial{0, 0, 0, 0, 0};
+    warp_reduce(p.sum_rho, p.sum_usqr, p.max_usqr, p.n_cells, p.n_nonfinite);
+    if (lane == 0) *out = p;
+  }
+}
+
+} // namespace olb_b200
+
+using namespace olb_b200;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+olb_b200_status fail(olb_b200_status code, const char* fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+olb_b200_status cuda_fail(cudaError_t e, const char* what)
+{
+  return fail(e == cudaErrorMemoryAllocation ? OLB_B200_ERR_OOM : OLB_B200_ERR_CUDA, "%s: %s (%s)",
+              what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+#define OLB_CUDA(call)                                                                             \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);                                            \
+  } while (0)
+
+bool is_fluid(int kind)
+{
+  return kind == K_BGK || kind == K_TRT || kind == K_SMAGORINSKY || kind == K_FORCED_BGK ||
+         kind == K_FORCED_TRT;
+}
+
+template <class R>
+DynDevice<R> make_device_params(int q, const olb_b200_dyn_params& in)
+{
+  // Cell-independent parts of each collision, evaluated in R with the
+  // reference's operation order (the host compiler does not contract).
+  DynDevice<R> d;
+  std::memset(&d, 0, sizeof d);
+  d.kind = in.kind;
+  const R omega = R(in.omega);
+  const R magic = R(in.magic);
+  d.omega = omega;
+  // collision::TRT  src/dynamics/collision.h:239 (double expression, rounded once)
+  d.omega_minus = R(double(R(1)) / (double(magic) / (double(R(1) / omega) - 0.5) + double(R(0.5))));
+  // detail::SmagorinskyEffectiveOmega  src/dynamics/collisionLES.h:67-71
+  const R s = R(in.smagorinsky);
+  R pre = s * s;
+  pre = pre * R(3);
+  pre = pre * R(3);
+  pre = pre * R(2);
+  d.smago_pre = R(double(pre) * std::sqrt(2.0));
+  d.tau_mol = R(1) / omega;
+  for (int e = 0; e < 3; ++e) {
+    d.force[e] = R(in.force[e]);
+    d.wall_u[e] = R(in.wall_u[e]);
+  }
+  // lbm::addExternalForce  src/dynamics/lbm.h:562
+  d.force_relax = R(1) - omega * R(0.5);
+  d.wall_rho = R(in.wall_rho);
+  // collision::NguyenLaddCorrection  src/dynamics/collision.h:341-343
+  for (int i = 0; i < q; ++i) {
+    int c[3];
+    R w;
+    if (q == 19) {
+      for (int e = 0; e < 3; ++e) c[e] = Lattice<19>::c(i, e);
+      w = R(Lattice<19>::wnum(i)) / R(Lattice<19>::wden(i));
+    } else {
+      for (int e = 0; e < 3; ++e) c[e] = Lattice<27>::c(i, e);
+      w = R(Lattice<27>::wnum(i)) / R(Lattice<27>::wden(i));
+    }
+    for (int e = 0; e < 3; ++e) {
+      R t = R(2) * d.wall_rho;
+      t = t * d.wall_u[e];
+      t = t * R(c[e]);
+      t = t * w;
+      t = t * R(3);
+      d.wall_term[i][e] = t;
+    }
+  }
+  return d;
+}
+
+} // namespace
+
+struct olb_b200_lattice {
+  olb_b200_desc desc{};
+  int q = 19;
+  size_t cells = 0;
+  size_t stride = 0;
+  size_t elem = 4;          // storage element size
+  size_t real = 4;          // compute element size (ABI element)
+  int device = 0;
+  Geometry g{};
+  void* pops = nullptr;
+  uint8_t* ids = nullptr;   // device, n bytes (masked lattices only)
+  void* table = nullptr;    // device DynDevice<R>[256]
+  alignas(16) unsigned char bulk[sizeof(DynDevice<double>)];  // host DynDevice<R>
+  int bulk_kind = K_BGK;
+  bool masked = true;
+  int n_entries = 0;
+  int parity = 0;           // 1 after an odd number of steps (shifted layout)
+  int64_t steps_done = 0;
+  void* scratch = nullptr;  // staging, 4 * cells * real bytes
+  StatPartial* partials = nullptr;
+  size_t n_partials = 0;
+  StatPartial* stat_dev = nullptr;
+  StatPartial* stat_host = nullptr;  // pinned
+  int block_z = 0, block_y = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  size_t device_bytes = 0;
+};
+
+namespace {
+
+olb_b200_status select_device(olb_b200_lattice* L)
+{
+  OLB_CUDA(cudaSetDevice(L->device));
+  return OLB_B200_OK;
+}
+
+void default_shape(const olb_b200_lattice* L, int& bz, int& by)
+{
+  // 256 threads: a full z-row segment per warp; rows stacked along y
+  bz = L->desc.nz >= 128 ? 128 : (L->desc.nz >= 64 ? 64 : 32);
+  by = 256 / bz;
+}
+
+template <class F>
+cudaError_t dispatch(const olb_b200_lattice* L, F&& f)
+{
+  switch (L->desc.storage) {
+  case OLB_B200_STORAGE_F32:
+    return L->q == 19 ? f(std::integral_constant<int, 19>{}, float{}, float{})
+                      : f(std::integral_constant<int, 27>{}, float{}, float{});
+  case OLB_B200_STORAGE_F64:
+    return L->q == 19 ? f(std::integral_constant<int, 19>{}, double{}, double{})
+                      : f(std::integral_constant<int, 27>{}, double{}, double{});
+  case OLB_B200_STORAGE_F16:
+    return L->q == 19 ? f(std::integral_constant<int, 19>{}, __half{}, float{})
+                      : f(std::integral_constant<int, 27>{}, __half{}, float{});
+  case OLB_B200_STORAGE_BF16:
+    return L->q == 19 ? f(std::integral_constant<int, 19>{}, __nv_bfloat16{}, float{})
+                      : f(std::integral_constant<int, 27>{}, __nv_bfloat16{}, float{});
+  }
+  return cudaErrorInvalidValue;
+}
+
+olb_b200_status ensure_partials(olb_b200_lattice* L)
+{
+  const dim3 grid = step_grid(L->g, L->block_z, L->block_y);
+  const size_t need = size_t(grid.x) * grid.y * grid.z;
+  if (need > L->n_partials) {
+    if (L->partials) cudaFree(L->partials);
+    L->partials = nullptr;
+    L->n_partials = 0;
+    OLB_CUDA(cudaMalloc(&L->partials, need * sizeof(StatPartial)));
+    L->n_partials = need;
+  }
+  return OLB_B200_OK;
+}
+
+olb_b200_status enqueue_steps(olb_b200_lattice* L, int steps, bool stats_last)
+{
+  for (int s = 0; s < steps; ++s) {
+    const bool stats = stats_last && s == steps - 1;
+    StepLaunch a;
+    a.pops = L->pops;
+    a.g = L->g;
+    a.ids = L->masked ? L->ids : nullptr;
+    a.table = L->table;
+    a.bulk = L->bulk;
+    a.partials = stats ? L->partials : nullptr;
+    a.block_z = L->block_z;
+    a.block_y = L->block_y;
+    a.stream = L->stream;
+    const bool odd = L->parity == 1;
+    cudaError_t e = dispatch(L, [&](auto qc, auto s_, auto r_) {
+      using S = decltype(s_);
+      using R = decltype(r_);
+      return launch_step<decltype(qc)::value, S, R>(a, L->bulk_kind, odd, L->masked, stats);
+    });
+    if (e != cudaSuccess) return cuda_fail(e, "step kernel launch");
+    L->parity ^= 1;
+    L->steps_done += 1;
+  }
+  return OLB_B200_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* olb_b200_last_error(void) { return g_last_error.c_str(); }
+
+int32_t olb_b200_abi_version(void) { return OLB_B200_ABI_VERSION; }
+
+const char* olb_b200_build_info(void)
+{
+  static const std::string info = std::string("openlb_b200 abi ") + std::to_string(OLB_B200_ABI_VERSION) +
+                                  "; nvcc " + std::to_string(__CUDACC_VER_MAJOR__) + "." +
+                                  std::to_string(__CUDACC_VER_MINOR__) +
+#ifdef OLB_B200_EXACT
+                                  "; sm_100a; -fmad=false (exact arithmetic build)";
+#else
+                                  "; sm_100a; -fmad=true";
+#endif
+  return info.c_str();
+}
+
+olb_b200_status olb_b200_create(const olb_b200_desc* desc, olb_b200_lattice** out)
+{
+  g_last_error.clear();
+  if (!desc || !out) return fail(OLB_B200_ERR_ARG, "create: null argument");
+  *out = nullptr;
+  if (desc->q != 19 && desc->q != 27) return fail(OLB_B200_ERR_ARG, "create: q must be 19 or 27, got %d", desc->q);
+  if (desc->nx < 1 || desc->ny < 1 || desc->nz < 1)
+    return fail(OLB_B200_ERR_ARG, "create: extent must be positive (%d,%d,%d)", desc->nx, desc->ny, desc->nz);
+  if (desc->storage < 0 || desc->storage > 3) return fail(OLB_B200_ERR_ARG, "create: unknown storage %d", desc->storage);
+  if (desc->reserved[0] || desc->reserved[1] || desc->reserved[2])
+    return fail(OLB_B200_ERR_ARG, "create: reserved fields must be zero");
+  const size_t cells = size_t(desc->nx) * desc->ny * desc->nz;
+  if (cells > (size_t(1) << 31)) return fail(OLB_B200_ERR_ARG, "create: %zu cells exceed 2^31", cells);
+  const size_t stride = (cells + 63) / 64 * 64;
+  if (stride * size_t(desc->q) > (size_t(1) << 40)) return fail(OLB_B200_ERR_ARG, "create: lattice too large");
+
+  auto* L = new olb_b200_lattice;
+  L->desc = *desc;
+  L->q = desc->q;
+  L->cells = cells;
+  L->stride = stride;
+  L->device = desc->device;
+  L->elem = desc->storage == OLB_B200_STORAGE_F64 ? 8 : (desc->storage == OLB_B200_STORAGE_F32 ? 4 : 2);
+  L->real = desc->storage == OLB_B200_STORAGE_F64 ? 8 : 4;
+  L->g = Geometry{desc->nx, desc->ny, desc->nz, uint32_t(stride)};
+  default_shape(L, L->block_z, L->block_y);
+
+  auto cleanup = [&](olb_b200_status st) {
+    olb_b200_destroy(L);
+    return st;
+  };
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return cleanup(st);
+#define OLB_CUDA_C(call)                                                                           \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return cleanup(cuda_fail(e_, #call));                                   \
+  } while (0)
+  OLB_CUDA_C(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
+  OLB_CUDA_C(cudaEventCreate(&L->ev0));
+  OLB_CUDA_C(cudaEventCreate(&L->ev1));
+  const size_t pop_bytes = stride * size_t(L->q) * L->elem;
+  OLB_CUDA_C(cudaMalloc(&L->pops, pop_bytes));
+  OLB_CUDA_C(cudaMemsetAsync(L->pops, 0, pop_bytes, L->stream));
+  OLB_CUDA_C(cudaMalloc(&L->ids, cells));
+  OLB_CUDA_C(cudaMemsetAsync(L->ids, 0, cells, L->stream));
+  OLB_CUDA_C(cudaMalloc(&L->table, 256 * sizeof(DynDevice<double>)));
+  OLB_CUDA_C(cudaMalloc(&L->scratch, 4 * cells * L->real));
+  OLB_CUDA_C(cudaMalloc(&L->stat_dev, sizeof(StatPartial)));
+  OLB_CUDA_C(cudaMallocHost(&L->stat_host, sizeof(StatPartial)));
+  L->device_bytes = pop_bytes + cells + 256 * sizeof(DynDevice<double>) + 4 * cells * L->real;
+  // default: every cell NoDynamics
+  olb_b200_dyn_params none{};
+  none.kind = OLB_B200_DYN_NONE;
+  none.wall_rho = 1.0;
+  st = olb_b200_set_dynamics(L, nullptr, &none, 1);
+  if (st != OLB_B200_OK) return cleanup(st);
+  OLB_CUDA_C(cudaStreamSynchronize(L->stream));
+#undef OLB_CUDA_C
+  *out = L;
+  return OLB_B200_OK;
+}
+
+void olb_b200_destroy(olb_b200_lattice* L)
+{
+  if (!L) return;
+  cudaSetDevice(L->device);
+  if (L->stream) cudaStreamSynchronize(L->stream);
+  if (L->pops) cudaFree(L->pops);
+  if (L->ids) cudaFree(L->ids);
+  if (L->table) cudaFree(L->table);
+  if (L->scratch) cudaFree(L->scratch);
+  if (L->partials) cudaFree(L->partials);
+  if (L->stat_dev) cudaFree(L->stat_dev);
+  if (L->stat_host) cudaFreeHost(L->stat_host);
+  if (L->ev0) cudaEventDestroy(L->ev0);
+  if (L->ev1) cudaEventDestroy(L->ev1);
+  if (L->stream) cudaStreamDestroy(L->stream);
+  delete L;
+}
+
+olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
+                                      const olb_b200_dyn_params* table, int32_t n_entries)
+{
+  g_last_error.clear();
+  if (!L || !table) return fail(OLB_B200_ERR_ARG, "set_dynamics: null argument");
+  if (n_entries < 1 || n_entries > 256)
+    return fail(OLB_B200_ERR_ARG, "set_dynamics: table needs 1..256 entries, got %d", n_entries);
+  int bulk = -1;
+  for (int k = 0; k < n_entries; ++k) {
+    const int kind = table[k].kind;
+    if (kind < OLB_B200_DYN_NONE || kind > OLB_B200_DYN_FORCED_TRT)
+      return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d has unknown kind %d", k, kind);
+    if (is_fluid(kind)) {
+      if (!(table[k].omega > 0.0 && table[k].omega < 2.0))
+        return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d omega %g outside (0,2)", k, table[k].omega);
+      if (bulk < 0) {
+        bulk = k;
+      } else if (table[bulk].kind != kind) {
+        return fail(OLB_B200_ERR_UNSUPPORTED,
+                    "set_dynamics: entries %d and %d use different fluid collisions (%d, %d); one "
+                    "fluid collision kind per lattice is supported", bulk, k, table[bulk].kind, kind);
+      }
+    }
+  }
+  bool uniform = ids == nullptr;
+  uint8_t first = 0;
+  if (ids) {
+    first = ids[0];
+    uniform = true;
+    for (size_t c = 0; c < L->cells; ++c) {
+      if (ids[c] >= n_entries)
+        return fail(OLB_B200_ERR_ARG, "set_dynamics: cell %zu has id %u >= %d entries", c, unsigned(ids[c]), n_entries);
+      uniform &= ids[c] == first;
+    }
+  }
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  // device table and the host copy of the bulk entry
+  const bool f64 = L->desc.storage == OLB_B200_STORAGE_F64;
+  std::vector<unsigned char> host(size_t(n_entries) * (f64 ? sizeof(DynDevice<double>) : sizeof(DynDevice<float>)));
+  for (int k = 0; k < n_entries; ++k) {
+    if (f64) {
+      auto d = make_device_params<double>(L->q, table[k]);
+      std::memcpy(host.data() + k * sizeof d, &d, sizeof d);
+    } else {
+      auto d = make_device_params<float>(L->q, table[k]);
+      std::memcpy(host.data() + k * sizeof d, &d, sizeof d);
+    }
+  }
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  OLB_CUDA(cudaMemcpy(L->table, host.data(), host.size(), cudaMemcpyHostToDevice));
+  if (ids) {
+    OLB_CUDA(cudaMemcpy(L->ids, ids, L->cells, cudaMemcpyHostToDevice));
+  } else {
+    OLB_CUDA(cudaMemset(L->ids, 0, L->cells));
+  }
+  const int bulk_entry = bulk >= 0 ? bulk : 0;
+  L->bulk_kind = bulk >= 0 ? table[bulk].kind : K_BGK;
+  const size_t esz = f64 ? sizeof(DynDevice<double>) : sizeof(DynDevice<float>);
+  std::memcpy(L->bulk, host.data() + bulk_entry * esz, esz);
+  // the unmasked kernel serves lattices where every cell uses one fluid entry
+  const int only = ids ? first : 0;
+  L->masked = !(uniform && is_fluid(table[only].kind));
+  if (!L->masked) {
+    std::memcpy(L->bulk, host.data() + only * esz, esz);
+  }
+  L->n_entries = n_entries;
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_set_populations(olb_b200_lattice* L, const void* host_pops)
+{
+  g_last_error.clear();
+  if (!L || !host_pops) return fail(OLB_B200_ERR_ARG, "set_populations: null argument");
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  const size_t col = L->cells * L->real;
+  const char* src = static_cast<const char*>(host_pops);
+  if (L->elem == L->real) {
+    for (int i = 0; i < L->q; ++i) {
+      OLB_CUDA(cudaMemcpyAsync(static_cast<char*>(L->pops) + size_t(i) * L->stride * L->elem,
+                               src + size_t(i) * col, col, cudaMemcpyHostToDevice, L->stream));
+    }
+  } else {
+    for (int i0 = 0; i0 < L->q; i0 += 4) {
+      const int i1 = std::min(L->q, i0 + 4);
+      OLB_CUDA(cudaMemcpyAsync(L->scratch, src + size_t(i0) * col, size_t(i1 - i0) * col,
+                               cudaMemcpyHostToDevice, L->stream));
+      cudaError_t e = dispatch(L, [&](auto qc, auto s_, auto r_) {
+        return launch_scatter<decltype(qc)::value, decltype(s_), decltype(r_)>(L->pops, L->g, L->scratch, i0, i1,
+                                                                              L->stream);
+      });
+      if (e != cudaSuccess) return cuda_fail(e, "scatter kernel");
+    }
+  }
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  L->parity = 0;
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_get_populations(olb_b200_lattice* L, void* host_pops)
+{
+  g_last_error.clear();
+  if (!L || !host_pops) return fail(OLB_B200_ERR_ARG, "get_populations: null argument");
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  const size_t col = L->cells * L->real;
+  char* dst = static_cast<char*>(host_pops);
+  if (L->elem == L->real && L->parity == 0) {
+    for (int i = 0; i < L->q; ++i) {
+      OLB_CUDA(cudaMemcpyAsync(dst + size_t(i) * col,
+                               static_cast<const char*>(L->pops) + size_t(i) * L->stride * L->elem, col,
+                               cudaMemcpyDeviceToHost, L->stream));
+    }
+  } else {
+    for (int i0 = 0; i0 < L->q; i0 += 4) {
+      const int i1 = std::min(L->q, i0 + 4);
+      cudaError_t e = dispatch(L, [&](auto qc, auto s_, auto r_) {
+        return launch_gather<decltype(qc)::value, decltype(s_), decltype(r_)>(L->pops, L->g, L->parity == 1,
+                                                                             L->scratch, i0, i1, L->stream);
+      });
+      if (e != cudaSuccess) return cuda_fail(e, "gather kernel");
+      OLB_CUDA(cudaMemcpyAsync(dst + size_t(i0) * col, L->scratch, size_t(i1 - i0) * col,
+                               cudaMemcpyDeviceToHost, L->stream));
+    }
+  }
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_collide_and_stream(olb_b200_lattice* L, int32_t steps, olb_b200_stats* stats)
+{
+  g_last_error.clear();
+  if (!L) return fail(OLB_B200_ERR_ARG, "collide_and_stream: null lattice");
+  if (steps < 0) return fail(OLB_B200_ERR_ARG, "collide_and_stream: negative step count %d", steps);
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  if (steps == 0) {
+    if (stats) std::memset(stats, 0, sizeof *stats);
+    return OLB_B200_OK;
+  }
+  if (stats) {
+    st = ensure_partials(L);
+    if (st != OLB_B200_OK) return st;
+  }
+  st = enqueue_steps(L, steps, stats != nullptr);
+  if (st != OLB_B200_OK) return st;
+  if (!stats) return OLB_B200_OK;
+  const dim3 grid = step_grid(L->g, L->block_z, L->block_y);
+  const size_t count = size_t(grid.x) * grid.y * grid.z;
+  reduce_partials_kernel<<<1, 1024, 0, L->stream>>>(L->partials, count, L->stat_dev);
+  OLB_CUDA(cudaGetLastError());
+  OLB_CUDA(cudaMemcpyAsync(L->stat_host, L->stat_dev, sizeof(StatPartial), cudaMemcpyDeviceToHost, L->stream));
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  const StatPartial p = *L->stat_host;
+  stats->sum_rho = p.sum_rho;
+  stats->sum_usqr = p.sum_usqr;
+  stats->max_usqr = p.max_usqr;
+  stats->n_cells = int64_t(p.n_cells);
+  // LatticeStatistics::reset: energy = 0.5 <|u|^2>, maxU = sqrt(max |u|^2)
+  // (src/core/latticeStatistics.hh:88-89)
+  stats->average_rho = p.n_cells ? p.sum_rho / double(p.n_cells) : 0.0;
+  stats->average_energy = p.n_cells ? 0.5 * p.sum_usqr / double(p.n_cells) : 0.0;
+  stats->max_u = std::sqrt(p.max_usqr);
+  stats->n_nonfinite = int64_t(p.n_nonfinite);
+  if (p.n_nonfinite) {
+    return fail(OLB_B200_ERR_DIVERGED, "collide_and_stream: %llu cells with non-finite density or "
+                "velocity after step %lld (simulation diverged)", p.n_nonfinite, (long long)L->steps_done);
+  }
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_get_moments(olb_b200_lattice* L, void* host_rho, void* host_u)
+{
+  g_last_error.clear();
+  if (!L || !host_rho || !host_u) return fail(OLB_B200_ERR_ARG, "get_moments: null argument");
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  char* rho_d = static_cast<char*>(L->scratch);
+  char* u_d = rho_d + L->cells * L->real;
+  cudaError_t e = dispatch(L, [&](auto qc, auto s_, auto r_) {
+    return launch_moments<decltype(qc)::value, decltype(s_), decltype(r_)>(
+      L->pops, L->g, L->parity == 1, L->ids, L->table, rho_d, u_d, L->stream);
+  });
+  if (e != cudaSuccess) return cuda_fail(e, "moments kernel");
+  OLB_CUDA(cudaMemcpyAsync(host_rho, rho_d, L->cells * L->real, cudaMemcpyDeviceToHost, L->stream));
+  OLB_CUDA(cudaMemcpyAsync(host_u, u_d, 3 * L->cells * L->real, cudaMemcpyDeviceToHost, L->stream));
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_synchronize(olb_b200_lattice* L)
+{
+  g_last_error.clear();
+  if (!L) return fail(OLB_B200_ERR_ARG, "synchronize: null lattice");
+  OLB_CUDA(cudaSetDevice(L->device));
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_time_steps(olb_b200_lattice* L, int32_t steps, float* ms)
+{
+  g_last_error.clear();
+  if (!L || !ms || steps < 1) return fail(OLB_B200_ERR_ARG, "time_steps: bad argument");
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  OLB_CUDA(cudaEventRecord(L->ev0, L->stream));
+  st = enqueue_steps(L, steps, false);
+  if (st != OLB_B200_OK) return st;
+  OLB_CUDA(cudaEventRecord(L->ev1, L->stream));
+  OLB_CUDA(cudaEventSynchronize(L->ev1));
+  OLB_CUDA(cudaEventElapsedTime(ms, L->ev0, L->ev1));
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_get_stream(olb_b200_lattice* L, void** stream)
+{
+  if (!L || !stream) return fail(OLB_B200_ERR_ARG, "get_stream: null argument");
+  *stream = L->stream;
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_get_info(olb_b200_lattice* L, int64_t* steps_done, int64_t* device_bytes,
+                                  int32_t* block_z, int32_t* block_y)
+{
+  if (!L) return fail(OLB_B200_ERR_ARG, "get_info: null lattice");
+  if (steps_done) *steps_done = L->steps_done;
+  if (device_bytes) *device_bytes = int64_t(L->device_bytes + L->n_partials * sizeof(StatPartial));
+  if (block_z) *block_z = L->block_z;
+  if (block_y) *block_y = L->block_y;
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_set_launch_shape(olb_b200_lattice* L, int32_t block_z, int32_t block_y)
+{
+  g_last_error.clear();
+  if (!L) return fail(OLB_B200_ERR_ARG, "set_launch_shape: null lattice");
+  if (block_z == 0 && block_y == 0) {
+    default_shape(L, L->block_z, L->block_y);
+    return OLB_B200_OK;
+  }
+  if (block_z < 32 || block_z % 32 != 0 || block_y < 1 || block_z * block_y > kStepThreads)
+    return fail(OLB_B200_ERR_ARG, "set_launch_shape: block (%d,%d) invalid: block_z a positive multiple "
+                "of 32, block_z*block_y <= %d", block_z, block_y, kStepThreads);
+  L->block_z = block_z;
+  L->block_y = block_y;
+  return OLB_B200_OK;
+}
+
+} // extern "C"

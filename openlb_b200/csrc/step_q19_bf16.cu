@@ -1,0 +1,3 @@
+// D3Q19, bfloat16 storage of scaled shifted populations, float arithmetic
+#include "launch_impl.cuh"
+OLB_B200_INSTANTIATE(19, __nv_bfloat16, float)

@@ -1,0 +1,388 @@
+"""Host-side mirror of OpenLB's lattice API for the B200 collide-and-stream.
+
+Two layers:
+
+* :class:`Lattice` — one lattice handle of the C ABI (``include/olb_b200.h``):
+  create, dynamics table, populations in/out, collide-and-stream, moments.
+* :class:`SuperGeometry` / :class:`SuperLattice` — the user-facing calls of an
+  OpenLB example with the reference's names and meaning
+  (``examples/laminar/cavity3dBenchmark/cavity3d.cpp:154-243``):
+  ``defineDynamics``, ``setParameter<OMEGA>``, ``defineU``, ``defineField<FORCE>``,
+  ``iniEquilibrium``, ``initialize``, ``collideAndStream``, ``getStatistics`` and
+  the Density3D / Velocity3D functors.
+
+Errors surface as :class:`openlb_b200._abi.OlbError` (a ``RuntimeError``), as
+OpenLB surfaces CUDA errors through ``std::runtime_error``.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from .descriptors import D3Q19, D3Q27, descriptor
+
+# ---------------------------------------------------------------------------
+# dynamics descriptions (the reference's dynamics aliases)
+
+
+@dataclass(frozen=True)
+class Dynamics:
+    """A dynamics alias and its per-dynamics parameters/fields."""
+    kind: int
+    omega: float | None = None
+    magic: float = 0.25
+    smagorinsky: float = 0.1
+    force: tuple = (0.0, 0.0, 0.0)
+    wall_u: tuple = (0.0, 0.0, 0.0)
+    wall_rho: float = 1.0
+
+    def params(self, omega_default: float | None = None) -> _abi.DynParams:
+        p = _abi.DynParams()
+        p.kind = self.kind
+        omega = self.omega if self.omega is not None else omega_default
+        p.omega = float(omega) if omega is not None else 1.0
+        p.magic = float(self.magic)
+        p.smagorinsky = float(self.smagorinsky)
+        for e in range(3):
+            p.force[e] = float(self.force[e])
+            p.wall_u[e] = float(self.wall_u[e])
+        p.wall_rho = float(self.wall_rho)
+        return p
+
+
+def NoDynamics() -> Dynamics:
+    return Dynamics(_abi.DYN_NONE)
+
+
+def BGKdynamics(omega: float | None = None) -> Dynamics:
+    return Dynamics(_abi.DYN_BGK, omega=omega)
+
+
+def TRTdynamics(omega: float | None = None, magic: float = 0.25) -> Dynamics:
+    return Dynamics(_abi.DYN_TRT, omega=omega, magic=magic)
+
+
+def ForcedTRTdynamics(omega: float | None = None, magic: float = 0.25, force=(0.0, 0.0, 0.0)) -> Dynamics:
+    return Dynamics(_abi.DYN_FORCED_TRT, omega=omega, magic=magic, force=tuple(force))
+
+
+def ForcedBGKdynamics(omega: float | None = None, force=(0.0, 0.0, 0.0)) -> Dynamics:
+    return Dynamics(_abi.DYN_FORCED_BGK, omega=omega, force=tuple(force))
+
+
+def SmagorinskyBGKdynamics(omega: float | None = None, smagorinsky: float = 0.1) -> Dynamics:
+    return Dynamics(_abi.DYN_SMAGORINSKY, omega=omega, smagorinsky=smagorinsky)
+
+
+def BounceBack(rho: float = 1.0) -> Dynamics:
+    return Dynamics(_abi.DYN_BOUNCE_BACK, wall_rho=rho)
+
+
+def BounceBackVelocity(u=(0.0, 0.0, 0.0), rho: float = 1.0) -> Dynamics:
+    return Dynamics(_abi.DYN_BOUNCE_BACK_VELOCITY, wall_u=tuple(u), wall_rho=rho)
+
+
+FLUID_KINDS = {_abi.DYN_BGK, _abi.DYN_TRT, _abi.DYN_SMAGORINSKY, _abi.DYN_FORCED_BGK, _abi.DYN_FORCED_TRT}
+
+# ---------------------------------------------------------------------------
+# block-level handle
+
+
+class Lattice:
+    """One lattice on one GPU, driven through the C ABI."""
+
+    def __init__(self, q: int, size, periodic=(False, False, False), storage: str = "f32",
+                 device: int = 0, variant: str = "fast"):
+        self._lib = _abi.load(variant)
+        self.q = int(q)
+        self.size = tuple(int(s) for s in size)
+        self.periodic = tuple(bool(p) for p in periodic)
+        self.storage = storage
+        self.dtype = np.float64 if storage == "f64" else np.float32
+        d = _abi.Desc()
+        d.q = self.q
+        d.nx, d.ny, d.nz = self.size
+        for e in range(3):
+            d.periodic[e] = int(self.periodic[e])
+        if storage not in _abi.STORAGE:
+            raise ValueError(f"unknown storage {storage!r}")
+        d.storage = _abi.STORAGE[storage]
+        d.device = int(device)
+        h = ctypes.c_void_p()
+        self._check(self._lib.olb_b200_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def n(self) -> int:
+        nx, ny, nz = self.size
+        return nx * ny * nz
+
+    def _check(self, status: int) -> None:
+        _abi.check(self._lib, status)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.olb_b200_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover - GC timing
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- configuration ------------------------------------------------------
+    def set_dynamics(self, table, ids: np.ndarray | None = None, omega: float | None = None) -> None:
+        params = (_abi.DynParams * len(table))()
+        for k, dyn in enumerate(table):
+            params[k] = dyn.params(omega)
+        ptr = None
+        if ids is not None:
+            ids = np.ascontiguousarray(ids, dtype=np.uint8).reshape(-1)
+            if ids.size != self.n:
+                raise ValueError(f"ids has {ids.size} entries, lattice has {self.n} cells")
+            ptr = ids.ctypes.data
+        self._check(self._lib.olb_b200_set_dynamics(self._h, ptr, params, len(table)))
+
+    def set_launch_shape(self, block_z: int, block_y: int) -> None:
+        self._check(self._lib.olb_b200_set_launch_shape(self._h, block_z, block_y))
+
+    # -- state --------------------------------------------------------------
+    def set_populations(self, pops: np.ndarray) -> None:
+        pops = np.ascontiguousarray(pops, dtype=self.dtype).reshape(-1)
+        if pops.size != self.q * self.n:
+            raise ValueError(f"populations need {self.q * self.n} values, got {pops.size}")
+        self._check(self._lib.olb_b200_set_populations(self._h, pops.ctypes.data))
+
+    def _out(self, arr, count):
+        if arr is None:
+            return np.empty(count, self.dtype)
+        if arr.dtype != self.dtype or arr.size != count or not arr.flags.c_contiguous:
+            raise ValueError(f"output buffer must be a contiguous {np.dtype(self.dtype).name}[{count}]")
+        return arr
+
+    def get_populations(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = self._out(out, self.q * self.n)
+        self._check(self._lib.olb_b200_get_populations(self._h, out.ctypes.data))
+        return out
+
+    def get_moments(self, out=None):
+        rho = self._out(None if out is None else out[0], self.n)
+        u = self._out(None if out is None else out[1], 3 * self.n)
+        self._check(self._lib.olb_b200_get_moments(self._h, rho.ctypes.data, u.ctypes.data))
+        return rho, u.reshape(3, self.n)
+
+    # -- stepping -----------------------------------------------------------
+    def collide_and_stream(self, steps: int = 1, stats: bool = False):
+        if stats:
+            st = _abi.Stats()
+            self._check(self._lib.olb_b200_collide_and_stream(self._h, int(steps), ctypes.byref(st)))
+            return st.as_dict()
+        self._check(self._lib.olb_b200_collide_and_stream(self._h, int(steps), None))
+        return None
+
+    def synchronize(self) -> None:
+        self._check(self._lib.olb_b200_synchronize(self._h))
+
+    def time_steps(self, steps: int) -> float:
+        ms = ctypes.c_float()
+        self._check(self._lib.olb_b200_time_steps(self._h, int(steps), ctypes.byref(ms)))
+        return float(ms.value)
+
+    def info(self) -> dict:
+        sd = ctypes.c_int64()
+        nb = ctypes.c_int64()
+        bz = ctypes.c_int32()
+        by = ctypes.c_int32()
+        self._check(self._lib.olb_b200_get_info(self._h, ctypes.byref(sd), ctypes.byref(nb),
+                                                ctypes.byref(bz), ctypes.byref(by)))
+        return {"steps_done": sd.value, "device_bytes": nb.value, "block_z": bz.value, "block_y": by.value}
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self._lib.olb_b200_get_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+
+# ---------------------------------------------------------------------------
+# OpenLB-style facade
+
+
+class SuperGeometry:
+    """Material numbers of a single-cuboid domain (z fastest, as OpenLB).
+
+    Mirrors ``SuperGeometry`` / ``BlockGeometry`` material access
+    (``src/geometry/blockGeometry.h:104-121``) and
+    ``CuboidDecomposition::setPeriodicity``.
+    """
+
+    def __init__(self, size, periodic=(False, False, False), material: int = 1):
+        self.size = tuple(int(s) for s in size)
+        self.periodic = tuple(bool(p) for p in periodic)
+        self.materials = np.full(self.size, int(material), dtype=np.int32)
+
+    def get(self, x, y, z) -> int:
+        return int(self.materials[x, y, z])
+
+    def set(self, x, y, z, material: int) -> None:
+        self.materials[x, y, z] = material
+
+    def rename(self, old: int, new: int, mask: np.ndarray | None = None) -> None:
+        sel = self.materials == old
+        if mask is not None:
+            sel &= mask
+        self.materials[sel] = new
+
+    def getNvoxel(self) -> int:
+        """Voxels with material != 0 (superGeometryStatistics3D.hh:318-328)."""
+        return int(np.count_nonzero(self.materials))
+
+
+def dynamics_table(materials: np.ndarray, dyn_of_material: dict, params: dict, force: dict,
+                   wall_u: dict, wall_rho: dict):
+    """Material numbers -> (dynamics table, per-cell uint8 ids).
+
+    One table entry per material present, in ascending material order; a
+    material without defineDynamics gets NoDynamics (the reference's default,
+    core/blockLattice.hh:393-416).  Lattice-wide parameters (OMEGA, MAGIC,
+    SMAGORINSKY) fill entries that do not set their own; FORCE / VELOCITY /
+    RHO fields are per material, as defineField / defineU / defineRho set them.
+    """
+    flat = np.asarray(materials).reshape(-1)
+    mats = np.unique(flat)
+    if len(mats) > 256:
+        raise ValueError("at most 256 distinct materials")
+    table, ids, index = [], np.zeros(flat.size, np.uint8), {}
+    omega = params.get("OMEGA")
+    for m in (int(v) for v in mats):
+        dyn = dyn_of_material.get(m, NoDynamics())
+        kw = {}
+        if dyn.kind in (_abi.DYN_FORCED_BGK, _abi.DYN_FORCED_TRT) and m in force:
+            kw["force"] = force[m]
+        if dyn.kind == _abi.DYN_BOUNCE_BACK_VELOCITY and m in wall_u:
+            kw["wall_u"] = wall_u[m]
+        if m in wall_rho:
+            kw["wall_rho"] = wall_rho[m]
+        if "MAGIC" in params:
+            kw["magic"] = params["MAGIC"]
+        if "SMAGORINSKY" in params:
+            kw["smagorinsky"] = params["SMAGORINSKY"]
+        if dyn.omega is None and omega is not None:
+            kw["omega"] = omega
+        if kw:
+            dyn = Dynamics(**{**dyn.__dict__, **kw})
+        if dyn.kind in FLUID_KINDS and dyn.omega is None:
+            raise ValueError(f"material {m}: OMEGA not set")
+        index[m] = len(table)
+        table.append(dyn)
+    for m, k in index.items():
+        ids[flat == m] = k
+    return table, ids
+
+
+class SuperLattice:
+    """The reference's ``SuperLattice<T,DESCRIPTOR>`` calls on the B200 platform."""
+
+    def __init__(self, geometry: SuperGeometry, lattice: str | int = "D3Q19", storage: str = "f32",
+                 device: int = 0, variant: str = "fast"):
+        self.geometry = geometry
+        self.descriptor = descriptor(lattice)
+        self.block = Lattice(self.descriptor.q, geometry.size, geometry.periodic, storage, device, variant)
+        self._dyn_of_material: dict[int, Dynamics] = {}
+        self._params = {"OMEGA": None}
+        self._force: dict[int, tuple] = {}
+        self._wall_u: dict[int, tuple] = {}
+        self._wall_rho: dict[int, float] = {}
+        self._pending_pops = np.zeros((self.descriptor.q, self.block.n), self.block.dtype)
+        self._initialized = False
+        self._statistics = None
+
+    # defineDynamics<DYNAMICS>(superGeometry, material)  superLattice.hh:286-291
+    def defineDynamics(self, geometry: SuperGeometry, material: int, dynamics: Dynamics) -> None:
+        self._dyn_of_material[int(material)] = dynamics
+
+    # setParameter<FIELD>(value)  blockLattice.h:562-572
+    def setParameter(self, name: str, value: float) -> None:
+        self._params[name] = float(value)
+
+    # defineField<FORCE>(superGeometry, material, value)
+    def defineForce(self, geometry: SuperGeometry, material: int, force) -> None:
+        self._force[int(material)] = tuple(float(f) for f in force)
+
+    # defineU(superGeometry, material, u) on BounceBackVelocity cells
+    def defineU(self, geometry: SuperGeometry, material: int, u) -> None:
+        self._wall_u[int(material)] = tuple(float(v) for v in u)
+
+    def defineRho(self, geometry: SuperGeometry, material: int, rho: float) -> None:
+        self._wall_rho[int(material)] = float(rho)
+
+    # iniEquilibrium(superGeometry, material, rhoF, uF)  superLattice.hh:542-577
+    def iniEquilibrium(self, geometry: SuperGeometry, material: int, rho, u) -> None:
+        sel = (geometry.materials.reshape(-1) == int(material))
+        n = self.block.n
+        rho_a = np.broadcast_to(np.asarray(rho, dtype=self.block.dtype), (n,))
+        u_a = np.asarray(u, dtype=self.block.dtype)
+        if u_a.shape == (3,):
+            u_a = np.broadcast_to(u_a[:, None], (3, n))
+        u_a = u_a.reshape(3, n)
+        feq = self.descriptor.equilibrium(rho_a[sel], u_a[:, sel], self.block.dtype)
+        self._pending_pops[:, sel] = feq
+        if self._initialized:
+            self.block.set_populations(self._pending_pops.reshape(-1))
+
+    def _table(self):
+        return dynamics_table(self.geometry.materials, self._dyn_of_material, self._params,
+                              self._force, self._wall_u, self._wall_rho)
+
+    # initialize()  superLattice.hh:190-204
+    def initialize(self) -> None:
+        table, ids = self._table()
+        self.block.set_dynamics(table, ids)
+        self.block.set_populations(self._pending_pops.reshape(-1))
+        self._initialized = True
+
+    # collideAndStream()  superLattice.hh:601-663
+    def collideAndStream(self, steps: int = 1, statistics: bool = False):
+        if not self._initialized:
+            self.initialize()
+        self._statistics = self.block.collide_and_stream(steps, stats=statistics)
+        return self._statistics
+
+    def getStatistics(self):
+        return self._statistics
+
+    # SuperLatticeDensity3D / SuperLatticeVelocity3D  latticeVelocity3D.hh:44-71
+    def getDensity(self) -> np.ndarray:
+        rho, _ = self.block.get_moments()
+        return rho.reshape(self.geometry.size)
+
+    def getVelocity(self) -> np.ndarray:
+        _, u = self.block.get_moments()
+        return u.reshape((3,) + self.geometry.size)
+
+    def getPopulations(self) -> np.ndarray:
+        return self.block.get_populations().reshape(self.descriptor.q, -1)
+
+    def setPopulations(self, pops: np.ndarray) -> None:
+        self._pending_pops[...] = np.asarray(pops).reshape(self.descriptor.q, -1)
+        if self._initialized:
+            self.block.set_populations(self._pending_pops.reshape(-1))
+
+    def close(self) -> None:
+        self.block.close()
+
+
+__all__ = [
+    "Dynamics", "NoDynamics", "BGKdynamics", "TRTdynamics", "ForcedTRTdynamics", "ForcedBGKdynamics",
+    "SmagorinskyBGKdynamics", "BounceBack", "BounceBackVelocity", "Lattice", "SuperGeometry",
+    "SuperLattice", "D3Q19", "D3Q27",
+]

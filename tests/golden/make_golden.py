@@ -1,0 +1,97 @@
+#!/usr/bin/env python3
+"""Generates the golden fixtures in this directory by running OpenLB itself.
+
+Each fixture is the output of the reference's own CPU_SISD build
+(oracle/_ref/olb_ref_sisd_*, built by oracle/ref/Makefile from the reference
+sources with OpenLB's public API) on a small seeded case: the inputs (geometry
+ids, dynamics table, initial populations) and the reference's populations,
+Density3D / Velocity3D fields and per-step LatticeStatistics after the stated
+number of collideAndStream steps.
+
+    python tests/golden/make_golden.py        # needs oracle/_ref (make -C oracle/ref)
+
+The C oracle is pinned against these fixtures in tests/test_oracle_golden.py.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT))
+
+from oracle import oracle as O  # noqa: E402
+from tests import cases as C  # noqa: E402
+
+
+def fixture_cases():
+    rng = np.random.default_rng(20261203)
+    out = []
+    # periodic boxes, every collision, random near-equilibrium state
+    for q in (19, 27):
+        for dtype in (np.float32, np.float64):
+            for kind in (O.BGK, O.TRT, O.SMAGORINSKY, O.FORCED_TRT):
+                case = C.periodic_case(q, (7, 6, 5), kind=kind)
+                f0 = C.random_state(q, case.n, dtype, rng)
+                variants = ["sisd"]
+                if q == 19 and dtype == np.float32:
+                    variants.append("nocse")
+                for variant in variants:
+                    name = f"periodic_q{q}_{np.dtype(dtype).name}_{O.KIND_NAMES[kind]}_{variant}"
+                    out.append((name, case, f0, 4, dtype, variant, False))
+    # lid-driven cavity: bounce-back walls, moving lid, rest start
+    for q in (19, 27):
+        for dtype in (np.float32, np.float64):
+            case = C.cavity_case(q, (9, 8, 7))
+            f0 = C.rest_state(q, case.n, dtype)
+            for variant in (["sisd", "nocse"] if (q == 19 and dtype == np.float32) else ["sisd"]):
+                out.append((f"cavity_q{q}_{np.dtype(dtype).name}_{variant}", case, f0, 25, dtype, variant, True))
+    # porous channel: Guo-forced TRT + bounce-back spheres, x periodic
+    case = C.porous_case(19, (12, 9, 8), np.random.default_rng(7), g=1e-4)
+    f0 = C.rest_state(19, case.n, np.float32)
+    for variant in ("sisd", "nocse"):
+        out.append((f"porous_q19_float32_{variant}", case, f0, 15, np.float32, variant, True))
+    # D3Q27 Smagorinsky channel with a square cylinder
+    case = C.channel_cylinder_case(27, (12, 8, 6), side=2)
+    n = case.n
+    u = np.zeros((3, n), np.float32)
+    u[0] = 0.05
+    f0 = O.equilibrium(27, np.ones(n, np.float32), u)
+    out.append(("channel_q27_float32_sisd", case, f0, 10, np.float32, "sisd", True))
+    return out
+
+
+def main():
+    manifest = {}
+    for name, case, f0, steps, dtype, variant, stats in fixture_cases():
+        ref = O.run_reference(case, steps, dtype, init=f0, variant=variant, stats=stats)
+        payload = {
+            "q": np.int32(case.q), "size": np.array(case.size, np.int32),
+            "periodic": np.array(case.periodic, np.int32), "steps": np.int32(steps),
+            "dyn_id": case.dyn_id if case.dyn_id is not None else np.zeros(case.n, np.uint8),
+            "table": np.array([[d.kind, d.omega, d.magic, d.smagorinsky, *d.force, *d.wall_u, d.wall_rho]
+                               for d in case.table], np.float64),
+            "init": f0, "pops": ref["pops"], "rho": ref["rho"], "u": ref["u"],
+        }
+        if stats:
+            payload["stats"] = ref["stats"]
+        path = HERE / f"{name}.npz"
+        np.savez_compressed(path, **payload)
+        manifest[name] = {"variant": variant, "dtype": np.dtype(dtype).name, "steps": steps,
+                          "sha256": hashlib.sha256(path.read_bytes()).hexdigest()}
+        print(name, path.stat().st_size)
+    gxx = subprocess.run(["g++", "--version"], capture_output=True, text=True).stdout.splitlines()[0]
+    (HERE / "MANIFEST.json").write_text(json.dumps(
+        {"generator": "tests/golden/make_golden.py", "reference_build": "oracle/ref/Makefile",
+         "compiler": gxx, "flags": "-O3 -std=c++20 -march=x86-64-v2 -ffp-contract=off -fopenmp",
+         "fixtures": manifest}, indent=1) + "\n")
+
+
+if __name__ == "__main__":
+    main()
