@@ -168,6 +168,34 @@ olb_b200_status olb_b200_get_info(olb_b200_lattice* lattice, int64_t* steps_done
  * block_z a multiple of 32).  0,0 selects the built-in default. */
 olb_b200_status olb_b200_set_launch_shape(olb_b200_lattice* lattice, int32_t block_z, int32_t block_y);
 
+/* Collide-and-stream on caller-owned device memory, allocating nothing.  This
+ * entry point has no counterpart in the reference.
+ *
+ * It is for callers that cannot let a plug-in allocate device memory: a host
+ * application that owns a fixed device-memory pool and forbids cudaMalloc /
+ * cudaFree outside it, or a service that sizes its memory once at start-up and
+ * must not allocate on the request path.  No lattice handle is involved (the
+ * handle allocates); the caller owns the populations:
+ *   device_pops  q columns of stride = round_up(nx*ny*nz, 64) elements of the
+ *                storage type, in this library's in-place (AA) order: after an
+ *                even number of steps it is the logical post-stream layout,
+ *                after an odd number each f_i(x) sits in column opp(i) at
+ *                x - c_i.  steps_done tells the call which of the two it is.
+ *   bulk         one fluid dynamics applied to every cell (no walls).
+ *   stats        NULL, or receives the last step's statistics (the call then
+ *                waits for the stream).
+ *   stream       a cudaStream_t, or NULL for the default stream.
+ * The statistics reduction uses a fixed 2.5 MiB __device__ scratch array that
+ * every GPU loading this library holds until exit; lattices needing more than
+ * 65536 reduction blocks (more than 256^3 cells) are rejected with
+ * OLB_B200_ERR_ARG when stats is requested.  The first call on each device
+ * looks up the scratch address and should come before any stream capture.
+ * Calls whose device work overlaps race on the shared scratch; serialise them. */
+olb_b200_status olb_b200_collide_and_stream_noalloc(const olb_b200_desc* desc, void* device_pops,
+                                                    int64_t steps_done,
+                                                    const olb_b200_dyn_params* bulk, int32_t steps,
+                                                    olb_b200_stats* stats, void* stream);
+
 /* Thread-local message of the last failed call on this thread ("" if none). */
 const char* olb_b200_last_error(void);
 

@@ -37,7 +37,7 @@ EXPORTED = [
     "olb_b200_get_populations", "olb_b200_collide_and_stream", "olb_b200_get_moments",
     "olb_b200_synchronize", "olb_b200_time_steps", "olb_b200_get_stream", "olb_b200_get_info",
     "olb_b200_set_launch_shape", "olb_b200_last_error", "olb_b200_abi_version",
-    "olb_b200_build_info",
+    "olb_b200_build_info", "olb_b200_collide_and_stream_noalloc",
 ]
 
 
@@ -130,6 +130,10 @@ def load(variant: str = "fast") -> ctypes.CDLL:
     lib.olb_b200_get_info.restype = st
     lib.olb_b200_set_launch_shape.argtypes = [P, ctypes.c_int32, ctypes.c_int32]
     lib.olb_b200_set_launch_shape.restype = st
+    lib.olb_b200_collide_and_stream_noalloc.argtypes = [ctypes.POINTER(Desc), P, ctypes.c_int64,
+                                                        ctypes.POINTER(DynParams), ctypes.c_int32,
+                                                        ctypes.POINTER(Stats), P]
+    lib.olb_b200_collide_and_stream_noalloc.restype = st
     lib.olb_b200_last_error.argtypes = []
     lib.olb_b200_last_error.restype = ctypes.c_char_p
     lib.olb_b200_abi_version.argtypes = []

@@ -156,6 +156,16 @@ DynDevice<R> make_device_params(int q, const olb_b200_dyn_params& in)
 
 } // namespace
 
+namespace olb_b200 {
+namespace detail {
+// entry points for other translation units of the library
+DynDevice<float> device_params_f32(int q, const olb_b200_dyn_params& in) { return make_device_params<float>(q, in); }
+DynDevice<double> device_params_f64(int q, const olb_b200_dyn_params& in) { return make_device_params<double>(q, in); }
+bool fluid_kind(int kind) { return is_fluid(kind); }
+void set_last_error(const std::string& message) { g_last_error = message; }
+} // namespace detail
+} // namespace olb_b200
+
 struct olb_b200_lattice {
   olb_b200_desc desc{};
   int q = 19;
