@@ -199,6 +199,8 @@ def run_ours(args, world, rank, local):
     lat = ob.Lattice(q, (n, n, n), (True, True, True), storage=storage, device=local)
     lat.set_dynamics([ob.BGKdynamics(omega=omega)])
     lat.set_populations(pops)
+    # pick the step-kernel variant and launch shape on this lattice (state restored)
+    tuning = lat.autotune(4)
     lat.collide_and_stream(args.warmup)
     lat.synchronize()
 
@@ -252,6 +254,7 @@ def run_ours(args, world, rank, local):
         "value": value, "ms_per_step": sec_max * 1e3 / args.steps, "clocks": clk.summary(),
         "e2e": e2e, "roofline": roofline, "gpu_launches": args.steps,
         "launch_shape": [info["block_z"], info["block_y"]], "cells": cells,
+        "tuning": {k: tuning[k] for k in ("variant", "cells_per_thread", "min_blocks_per_sm", "candidates")},
     }
 
 
@@ -340,6 +343,7 @@ def main():
     line.update({"value": res["value"], "ms_per_step": res["ms_per_step"], "e2e": res["e2e"],
                  "roofline": res["roofline"], "clocks": res["clocks"], "gpu_launches": res["gpu_launches"]})
     line["config"]["launch_shape"] = res["launch_shape"]
+    line["config"]["step_variant"] = res["tuning"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
         ref, err = run_reference_cpu(args.n, 30, 2, threads)

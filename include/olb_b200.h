@@ -164,9 +164,32 @@ olb_b200_status olb_b200_get_stream(olb_b200_lattice* lattice, void** stream);
 olb_b200_status olb_b200_get_info(olb_b200_lattice* lattice, int64_t* steps_done,
                                   int64_t* device_bytes, int32_t* block_z, int32_t* block_y);
 
-/* Launch shape of the step kernel (threads along z and y, product <= 512,
+/* Launch shape of the step kernel (threads along z and y, product <= 256,
  * block_z a multiple of 32).  0,0 selects the built-in default. */
 olb_b200_status olb_b200_set_launch_shape(olb_b200_lattice* lattice, int32_t block_z, int32_t block_y);
+
+/* Step-kernel tuning.  The library compiles a few variants of the step kernel
+ * (cells per thread x register cap) that compute identical results and differ
+ * only in speed; it picks a default per lattice class.  The reference has no
+ * counterpart (its kernels launch 32-thread blocks, gpu/cuda/operator.hh:424-427). */
+typedef struct {
+  int32_t variant;            /* index of the step-kernel variant */
+  int32_t cells_per_thread;
+  int32_t min_blocks_per_sm;  /* register cap = 65536 / (256 * min_blocks_per_sm) */
+  int32_t block_z, block_y;
+  int32_t tuned;              /* 1 if chosen by olb_b200_autotune */
+  int32_t candidates;         /* (variant, shape) pairs timed by the last autotune */
+  float ms_per_step;          /* best time per step measured by autotune, else 0 */
+} olb_b200_tuning;
+
+/* Times every (variant, launch shape) pair on this lattice for trial_steps
+ * steps each (0: 4) and keeps the fastest.  The lattice state is copied to a
+ * temporary device buffer first and restored afterwards, so the simulation does
+ * not advance.  Synchronous. */
+olb_b200_status olb_b200_autotune(olb_b200_lattice* lattice, int32_t trial_steps, olb_b200_tuning* out);
+olb_b200_status olb_b200_get_tuning(olb_b200_lattice* lattice, olb_b200_tuning* out);
+/* Selects a variant explicitly (-1: the library's default for this lattice). */
+olb_b200_status olb_b200_set_step_variant(olb_b200_lattice* lattice, int32_t variant);
 
 /* Collide-and-stream on caller-owned device memory, allocating nothing.  This
  * entry point has no counterpart in the reference.

@@ -37,7 +37,8 @@ EXPORTED = [
     "olb_b200_get_populations", "olb_b200_collide_and_stream", "olb_b200_get_moments",
     "olb_b200_synchronize", "olb_b200_time_steps", "olb_b200_get_stream", "olb_b200_get_info",
     "olb_b200_set_launch_shape", "olb_b200_last_error", "olb_b200_abi_version",
-    "olb_b200_build_info", "olb_b200_collide_and_stream_noalloc",
+    "olb_b200_build_info", "olb_b200_collide_and_stream_noalloc", "olb_b200_autotune",
+    "olb_b200_get_tuning", "olb_b200_set_step_variant",
 ]
 
 
@@ -76,6 +77,16 @@ class Stats(ctypes.Structure):
                 ("max_usqr", ctypes.c_double), ("n_cells", ctypes.c_int64),
                 ("average_rho", ctypes.c_double), ("average_energy", ctypes.c_double),
                 ("max_u", ctypes.c_double), ("n_nonfinite", ctypes.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("variant", ctypes.c_int32), ("cells_per_thread", ctypes.c_int32),
+                ("min_blocks_per_sm", ctypes.c_int32), ("block_z", ctypes.c_int32),
+                ("block_y", ctypes.c_int32), ("tuned", ctypes.c_int32), ("candidates", ctypes.c_int32),
+                ("ms_per_step", ctypes.c_float)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -134,6 +145,12 @@ def load(variant: str = "fast") -> ctypes.CDLL:
                                                         ctypes.POINTER(DynParams), ctypes.c_int32,
                                                         ctypes.POINTER(Stats), P]
     lib.olb_b200_collide_and_stream_noalloc.restype = st
+    lib.olb_b200_autotune.argtypes = [P, ctypes.c_int32, ctypes.POINTER(Tuning)]
+    lib.olb_b200_autotune.restype = st
+    lib.olb_b200_get_tuning.argtypes = [P, ctypes.POINTER(Tuning)]
+    lib.olb_b200_get_tuning.restype = st
+    lib.olb_b200_set_step_variant.argtypes = [P, ctypes.c_int32]
+    lib.olb_b200_set_step_variant.restype = st
     lib.olb_b200_last_error.argtypes = []
     lib.olb_b200_last_error.restype = ctypes.c_char_p
     lib.olb_b200_abi_version.argtypes = []

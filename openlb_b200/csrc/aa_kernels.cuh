@@ -34,8 +34,28 @@ namespace olb_b200 {
 
 struct Geometry {
   int32_t nx, ny, nz;
-  uint32_t stride;  // column length in elements
+  uint32_t stride;  // column length in storage elements
+  int32_t paired;   // 1: 16-bit storage with cells x and x + nx/2 in one 4-byte element
 };
+
+// Scalar slot of a cell within a population column.
+//   natural layout: (x*ny + y)*nz + z
+//   paired layout (16-bit storage, nx even): element ((x mod nx/2)*ny + y)*nz + z
+//   holds cell x in its low half and cell x + nx/2 in its high half, so the
+//   slot is 2*element + (x >= nx/2).  Shifts along y and z keep elements
+//   aligned; only the x seam swaps the halves.
+OLB_HD uint32_t cell_slot(const Geometry& g, int x, int y, int z)
+{
+  if (!g.paired) {
+    return (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
+  }
+  const int nxh = g.nx >> 1;
+  const int hi = x >= nxh;
+  const uint32_t e = (uint32_t(hi ? x - nxh : x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
+  return 2u * e + uint32_t(hi);
+}
+
+OLB_HD int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
 // per-block partial of the fused statistics reduction (FP64)
 struct StatPartial {
@@ -148,31 +168,36 @@ OLB_DEV void block_stats(double a, double b, double m, unsigned long long n, uns
 // ---------------------------------------------------------------------------
 // the step kernel
 
-// Cells per thread (along y, blockDim.y rows apart) and the launch bounds of
-// the step kernel.  All loads of a thread's cells are issued before any of
-// them is collided, so CELLS_PER_THREAD multiplies the bytes each thread keeps
-// in flight — the quantity that bounds this HBM-streaming kernel.
-#ifndef OLB_B200_CELLS_PER_THREAD
-#define OLB_B200_CELLS_PER_THREAD 1
+// Step-kernel variants: cells per thread (along y, blockDim.y rows apart) and
+// the register cap (__launch_bounds__(kStepThreads, min_blocks)).  All loads of
+// a thread's cells are issued before any of them is collided, so more cells
+// per thread — or more resident warps — means more bytes in flight per SM, the
+// quantity that bounds this HBM-streaming kernel.  Which variant is fastest
+// depends on the lattice, the storage type and the mask; the library picks a
+// default per lattice and can time all of them (olb_b200_autotune).  Every
+// variant performs the same arithmetic on every cell, so results are
+// independent of the choice.
+constexpr int kStepThreads = 256;
+struct StepVariant {
+  int cells_per_thread;
+  int min_blocks;
+};
+#ifdef OLB_B200_SINGLE_VARIANT
+// builds that only check arithmetic compile one variant; every id maps to it
+constexpr StepVariant kStepVariants[] = {{1, 3}, {1, 3}, {1, 3}, {1, 3}};
+#else
+constexpr StepVariant kStepVariants[] = {{1, 3}, {1, 4}, {2, 2}, {2, 3}};
 #endif
-#ifndef OLB_B200_STEP_THREADS
-#define OLB_B200_STEP_THREADS 256
-#endif
-#ifndef OLB_B200_STEP_MIN_BLOCKS
-#define OLB_B200_STEP_MIN_BLOCKS 2
-#endif
-constexpr int kCellsPerThread = OLB_B200_CELLS_PER_THREAD;
-constexpr int kStepThreads = OLB_B200_STEP_THREADS;
+constexpr int kNumStepVariants = 4;
 
-template <int Q, class S, class R, int KIND, bool ODD, bool MASKED, bool STATS>
-__global__ void __launch_bounds__(OLB_B200_STEP_THREADS, OLB_B200_STEP_MIN_BLOCKS)
+template <int Q, class S, class R, int KIND, bool ODD, bool MASKED, bool STATS, int CPT, int MINB>
+__global__ void __launch_bounds__(kStepThreads, MINB)
 aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict__ ids,
                const DynDevice<R>* __restrict__ table, const DynDevice<R> bulk,
                StatPartial* __restrict__ partials)
 {
   using L = Lattice<Q>;
   using ST = Store<S, R>;
-  constexpr int CPT = kCellsPerThread;
   const int z = blockIdx.x * blockDim.x + threadIdx.x;
   const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
   const int x = blockIdx.z;
@@ -280,6 +305,228 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict
   }
 }
 
+// ---------------------------------------------------------------------------
+// the step kernel on the paired 16-bit layout
+//
+// Each thread updates the two cells of one 4-byte element, (x', y, z) and
+// (x' + nx/2, y, z), with one aligned 32-bit load and one aligned 32-bit store
+// per population — a warp moves 128 B per instruction instead of 64 B.  The
+// grid's z dimension walks x' in [0, nx/2); a neighbour across the x seam is
+// the element on the other side with its halves swapped, a condition that is
+// uniform per block.  Cells of a pair may have different dynamics; full-way
+// bounce-back cells then apply their swap in registers (it writes back what
+// it read, so the result is the same as skipping them).
+
+template <class S> struct Pair;
+template <> struct Pair<__half> {
+  using T = __half2;
+  OLB_DEV static float2 to_float2(T v) { return __half22float2(v); }
+  OLB_DEV static T from_floats(float lo, float hi) { return __floats2half2_rn(lo, hi); }
+};
+template <> struct Pair<__nv_bfloat16> {
+  using T = __nv_bfloat162;
+  OLB_DEV static float2 to_float2(T v) { return __bfloat1622float2(v); }
+  OLB_DEV static T from_floats(float lo, float hi) { return __floats2bfloat162_rn(lo, hi); }
+};
+
+struct PairNeighbours {
+  uint32_t xo[3], yo[3], zo[3];
+  bool swap[3];
+  OLB_DEV PairNeighbours(const Geometry& g, int xp, int y, int z)
+  {
+    const int nxh = g.nx >> 1;
+    const uint32_t sxy = uint32_t(g.ny) * uint32_t(g.nz);
+    xo[0] = uint32_t(xp == 0 ? nxh - 1 : xp - 1) * sxy;
+    xo[1] = uint32_t(xp) * sxy;
+    xo[2] = uint32_t(xp == nxh - 1 ? 0 : xp + 1) * sxy;
+    swap[0] = xp == 0;
+    swap[1] = false;
+    swap[2] = xp == nxh - 1;
+    yo[0] = uint32_t(y == 0 ? g.ny - 1 : y - 1) * uint32_t(g.nz);
+    yo[1] = uint32_t(y) * uint32_t(g.nz);
+    yo[2] = uint32_t(y == g.ny - 1 ? 0 : y + 1) * uint32_t(g.nz);
+    zo[0] = uint32_t(z == 0 ? g.nz - 1 : z - 1);
+    zo[1] = uint32_t(z);
+    zo[2] = uint32_t(z == g.nz - 1 ? 0 : z + 1);
+  }
+  template <int DX, int DY, int DZ>
+  OLB_DEV uint32_t at() const { return xo[DX + 1] + yo[DY + 1] + zo[DZ + 1]; }
+};
+
+// collision of one cell of a pair by its runtime kind (masked lattices)
+template <class L, int KIND, bool MASKED>
+OLB_DEV bool collide_any(float (&f)[L::q], int kind, const DynDevice<float>* e, const DynDevice<float>& bulk,
+                         float& st_rho, float& st_usqr)
+{
+  if (kind == KIND) {
+    if constexpr (MASKED) {
+      DynDevice<float> q;
+      q.omega = __ldg(&e->omega);
+      q.omega_minus = __ldg(&e->omega_minus);
+      q.smago_pre = __ldg(&e->smago_pre);
+      q.tau_mol = __ldg(&e->tau_mol);
+      q.force[0] = __ldg(&e->force[0]);
+      q.force[1] = __ldg(&e->force[1]);
+      q.force[2] = __ldg(&e->force[2]);
+      q.force_relax = __ldg(&e->force_relax);
+      collide_bulk<L, KIND>(f, q, st_rho, st_usqr);
+    } else {
+      collide_bulk<L, KIND>(f, bulk, st_rho, st_usqr);
+    }
+    return true;
+  }
+  if constexpr (MASKED) {
+    if (kind == K_BOUNCE_BACK) {
+      revert<L>(f);
+    } else if (kind == K_BOUNCE_BACK_VELOCITY) {
+      revert<L>(f);
+      static_for<1, L::q>([&](auto i) {
+        f[i] += __ldg(&e->wall_term[i][0]);
+        f[i] += __ldg(&e->wall_term[i][1]);
+        f[i] += __ldg(&e->wall_term[i][2]);
+      });
+      st_rho = __ldg(&e->wall_rho);
+      const float wu[3] = {__ldg(&e->wall_u[0]), __ldg(&e->wall_u[1]), __ldg(&e->wall_u[2])};
+      st_usqr = norm_sqr(wu);
+      return true;
+    }
+  }
+  return false;  // NoDynamics / bounce-back: no statistic
+}
+
+template <int Q, class S, int KIND, bool ODD, bool MASKED, bool STATS, int CPT, int MINB>
+__global__ void __launch_bounds__(kStepThreads, MINB)
+aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8_t* __restrict__ ids,
+                      const DynDevice<float>* __restrict__ table, const DynDevice<float> bulk,
+                      StatPartial* __restrict__ partials)
+{
+  using L = Lattice<Q>;
+  using P = Pair<S>;
+  using T = typename P::T;
+  T* __restrict__ pops = reinterpret_cast<T*>(pops_scalar);
+  const uint32_t pstride = g.stride >> 1;  // elements per column
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
+  const int xp = blockIdx.z;
+  const uint32_t half_cells = uint32_t(g.nx >> 1) * uint32_t(g.ny) * uint32_t(g.nz);
+
+  double s_rho = 0., s_usqr = 0., s_max = 0.;
+  unsigned long long s_n = 0, s_nf = 0;
+
+  // the loaded pairs stay packed (low half = cell x', high half = x' + nx/2):
+  // one 32-bit register per population for both cells
+  T raw[CPT][Q];
+  int kind_lo[CPT], kind_hi[CPT];
+  bool go[CPT];
+  uint32_t e[CPT];
+  const DynDevice<float>* p_lo[CPT];
+  const DynDevice<float>* p_hi[CPT];
+
+  static_for<0, CPT>([&](auto k) {
+    const int y = y0 + k.value * int(blockDim.y);
+    go[k] = z < g.nz && y < g.ny;
+    kind_lo[k] = kind_hi[k] = KIND;
+    p_lo[k] = p_hi[k] = &bulk;
+    e[k] = 0;
+    if (go[k]) {
+      e[k] = (uint32_t(xp) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
+      if constexpr (MASKED) {
+        p_lo[k] = table + ids[e[k]];
+        p_hi[k] = table + ids[e[k] + half_cells];
+        kind_lo[k] = __ldg(&p_lo[k]->kind);
+        kind_hi[k] = __ldg(&p_hi[k]->kind);
+      }
+      // two bounce-back cells: nothing to do (AA no-op)
+      go[k] = !(kind_lo[k] == K_BOUNCE_BACK && kind_hi[k] == K_BOUNCE_BACK);
+    }
+    if (go[k]) {
+      PairNeighbours nb(g, xp, y, z);
+      static_for<0, Q>([&](auto i) {
+        if constexpr (!ODD) {
+          raw[k][i] = pops[size_t(i.value) * pstride + e[k]];
+        } else {
+          constexpr int o = L::opp(i);
+          const uint32_t src = nb.template at<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>();
+          const T v = pops[size_t(o) * pstride + src];
+          if (nb.swap[1 - L::c(i, 0)]) {
+            raw[k][i].x = v.y;
+            raw[k][i].y = v.x;
+          } else {
+            raw[k][i] = v;
+          }
+        }
+      });
+    }
+  });
+
+  static_for<0, CPT>([&](auto k) {
+    if (!go[k]) return;
+    const int y = y0 + k.value * int(blockDim.y);
+    // in the odd step the value read for population i is column opp(i)'s storage
+    auto unpack = [&](auto half_tag) {
+      float f[Q];
+      static_for<0, Q>([&](auto i) {
+        constexpr int col = ODD ? L::opp(i) : i.value;
+        constexpr float inv = 1.f / storage_scale<L>(col);
+        const float2 fv = P::to_float2(raw[k][i]);
+        f[i] = (decltype(half_tag)::value ? fv.y : fv.x) * inv;
+      });
+      return f;
+    };
+    auto cell = [&](auto half_tag, int kind, const DynDevice<float>* pe) {
+      constexpr bool HI = decltype(half_tag)::value;
+      float f[Q];
+      static_for<0, Q>([&](auto i) {
+        constexpr int col = ODD ? L::opp(i) : i.value;
+        constexpr float inv = 1.f / storage_scale<L>(col);
+        const float2 fv = P::to_float2(raw[k][i]);
+        f[i] = (HI ? fv.y : fv.x) * inv;
+      });
+      float r = 0.f, u2 = 0.f;
+      const bool counted = collide_any<L, KIND, MASKED>(f, kind, pe, bulk, r, u2);
+      // repack: the written value is population i in column (ODD ? i : opp(i))
+      static_for<0, Q>([&](auto i) {
+        constexpr int col = ODD ? i.value : L::opp(i);
+        constexpr float sc = storage_scale<L>(col);
+        const T packed = P::from_floats(f[i] * sc, f[i] * sc);
+        if constexpr (HI) {
+          raw[k][i].y = packed.y;
+        } else {
+          raw[k][i].x = packed.x;
+        }
+      });
+      if constexpr (STATS) {
+        if (counted) {
+          const double rr = r, uu = u2;
+          if (isfinite(rr) && isfinite(uu)) { s_rho += rr; s_usqr += uu; s_max = fmax(s_max, uu); s_n += 1; }
+          else { s_nf += 1; }
+        }
+      }
+    };
+    (void)unpack;
+    cell(std::integral_constant<bool, false>{}, kind_lo[k], p_lo[k]);
+    cell(std::integral_constant<bool, true>{}, kind_hi[k], p_hi[k]);
+    PairNeighbours nb(g, xp, y, z);
+    static_for<0, Q>([&](auto i) {
+      if constexpr (!ODD) {
+        constexpr int o = L::opp(i);
+        pops[size_t(o) * pstride + e[k]] = raw[k][i];
+      } else {
+        const uint32_t dst = nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>();
+        T v = raw[k][i];
+        if (nb.swap[1 + L::c(i, 0)]) {
+          v.x = raw[k][i].y;
+          v.y = raw[k][i].x;
+        }
+        pops[size_t(i.value) * pstride + dst] = v;
+      }
+    });
+  });
+  if constexpr (STATS) {
+    block_stats(s_rho, s_usqr, s_max, s_n, s_nf, partials);
+  }
+}
+
 // Deterministic second pass over the per-block partials (one block).
 __global__ void reduce_partials_kernel(const StatPartial* __restrict__ parts, size_t count,
                                        StatPartial* __restrict__ out);
@@ -287,18 +534,18 @@ __global__ void reduce_partials_kernel(const StatPartial* __restrict__ parts, si
 // ---------------------------------------------------------------------------
 // logical-layout gather / scatter and moments
 
-// Logical population i at cell x: natural column after an even number of
-// steps, else column opp(i) at x - c_i.
+// Logical population i at cell (x,y,z): column i at the cell after an even
+// number of steps, else column opp(i) at (x,y,z) - c_i (per-axis wrap).
 template <int Q, class S, class R, int I>
-OLB_DEV R logical_pop(const S* __restrict__ pops, const Geometry& g, const Neighbours& nb,
-                      uint32_t n, bool shifted)
+OLB_DEV R logical_pop(const S* __restrict__ pops, const Geometry& g, int x, int y, int z, bool shifted)
 {
   using L = Lattice<Q>;
   if (!shifted) {
-    return Store<S, R>::template load<L, I>(pops + size_t(I) * g.stride + n);
+    return Store<S, R>::template load<L, I>(pops + size_t(I) * g.stride + cell_slot(g, x, y, z));
   }
   constexpr int o = L::opp(I);
-  const uint32_t src = nb.template at<-L::c(I, 0), -L::c(I, 1), -L::c(I, 2)>();
+  const uint32_t src = cell_slot(g, wrap(x - L::c(I, 0), g.nx), wrap(y - L::c(I, 1), g.ny),
+                                 wrap(z - L::c(I, 2), g.nz));
   return Store<S, R>::template load<L, o>(pops + size_t(o) * g.stride + src);
 }
 
@@ -312,26 +559,29 @@ __global__ void gather_logical_kernel(const S* __restrict__ pops, const Geometry
   if (z >= g.nz || y >= g.ny) return;
   const uint32_t n = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
   const size_t cells = size_t(g.nx) * g.ny * g.nz;
-  Neighbours nb(g, x, y, z);
   static_for<0, Q>([&](auto i) {
     if (i.value >= i_begin && i.value < i_end) {
-      out[size_t(i.value - i_begin) * cells + n] = logical_pop<Q, S, R, i.value>(pops, g, nb, n, shifted);
+      out[size_t(i.value - i_begin) * cells + n] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted);
     }
   });
 }
 
-// natural-order write of logical populations (resets the AA parity)
+// write of logical populations in the unshifted order (resets the AA parity)
 template <int Q, class S, class R>
 __global__ void scatter_natural_kernel(S* __restrict__ pops, const Geometry g,
                                        const R* __restrict__ in, int i_begin, int i_end)
 {
   using L = Lattice<Q>;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.nz || y >= g.ny) return;
+  const uint32_t n = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
   const size_t cells = size_t(g.nx) * g.ny * g.nz;
-  const size_t n = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
-  if (n >= cells) return;
+  const uint32_t slot = cell_slot(g, x, y, z);
   static_for<0, Q>([&](auto i) {
     if (i.value >= i_begin && i.value < i_end) {
-      Store<S, R>::template store<L, i.value>(pops + size_t(i.value) * g.stride + n,
+      Store<S, R>::template store<L, i.value>(pops + size_t(i.value) * g.stride + slot,
                                               in[size_t(i.value - i_begin) * cells + n]);
     }
   });
@@ -356,9 +606,8 @@ __global__ void moments_kernel(const S* __restrict__ pops, const Geometry g, boo
   R rho, u[3];
   if (kind == K_BGK || kind == K_TRT || kind == K_SMAGORINSKY || kind == K_FORCED_BGK ||
       kind == K_FORCED_TRT) {
-    Neighbours nb(g, x, y, z);
     R f[Q];
-    static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, nb, n, shifted); });
+    static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted); });
     if (kind == K_FORCED_BGK || kind == K_FORCED_TRT) {
       const R gg[3] = {p->force[0], p->force[1], p->force[2]};
       compute_rho_u_forced<L>(f, gg, rho, u);
@@ -389,6 +638,7 @@ struct StepLaunch {
   const void* bulk;        // host DynDevice<R>
   StatPartial* partials;   // device, gridDim product entries
   int block_z, block_y;
+  int variant;             // index into kStepVariants
   cudaStream_t stream;
 };
 
@@ -407,10 +657,10 @@ template <int Q, class S, class R>
 cudaError_t launch_moments(const void* pops, const Geometry& g, bool shifted, const uint8_t* ids,
                            const void* table, void* rho, void* u, cudaStream_t stream);
 
-inline dim3 step_grid(const Geometry& g, int bz, int by)
+inline dim3 step_grid(const Geometry& g, int bz, int by, int cells_per_thread)
 {
-  const int rows = by * kCellsPerThread;
-  return dim3((g.nz + bz - 1) / bz, (g.ny + rows - 1) / rows, g.nx);
+  const int rows = by * cells_per_thread;
+  return dim3((g.nz + bz - 1) / bz, (g.ny + rows - 1) / rows, g.paired ? g.nx / 2 : g.nx);
 }
 
 // grid of the gather / moments kernels (one cell per thread)

@@ -4,21 +4,33 @@
 // in parallel.
 #pragma once
 
+#include <type_traits>
+
 #include "aa_kernels.cuh"
 
 namespace olb_b200 {
 
-template <int Q, class S, class R, int KIND>
-static cudaError_t launch_step_kind(const StepLaunch& a, bool odd, bool masked, bool stats)
+template <int Q, class S, class R, int KIND, int CPT, int MINB>
+static cudaError_t launch_step_variant(const StepLaunch& a, bool odd, bool masked, bool stats)
 {
   const dim3 block(a.block_z, a.block_y);
-  const dim3 grid = step_grid(a.g, a.block_z, a.block_y);
+  const dim3 grid = step_grid(a.g, a.block_z, a.block_y, CPT);
   S* pops = static_cast<S*>(a.pops);
   const DynDevice<R>* table = static_cast<const DynDevice<R>*>(a.table);
   const DynDevice<R>& bulk = *static_cast<const DynDevice<R>*>(a.bulk);
-#define OLB_LAUNCH(O, M, ST)                                                                  \
-  aa_step_kernel<Q, S, R, KIND, O, M, ST><<<grid, block, 0, a.stream>>>(pops, a.g, a.ids, table, \
-                                                                        bulk, a.partials)
+  constexpr bool kHalf = std::is_same_v<S, __half> || std::is_same_v<S, __nv_bfloat16>;
+#define OLB_LAUNCH(O, M, ST)                                                                       \
+  do {                                                                                             \
+    if constexpr (kHalf) {                                                                         \
+      if (a.g.paired) {                                                                            \
+        aa_step_paired_kernel<Q, S, KIND, O, M, ST, CPT, MINB><<<grid, block, 0, a.stream>>>(      \
+          pops, a.g, a.ids, table, bulk, a.partials);                                              \
+        break;                                                                                     \
+      }                                                                                            \
+    }                                                                                              \
+    aa_step_kernel<Q, S, R, KIND, O, M, ST, CPT, MINB><<<grid, block, 0, a.stream>>>(              \
+      pops, a.g, a.ids, table, bulk, a.partials);                                                  \
+  } while (0)
   if (odd) {
     if (masked) {
       if (stats) OLB_LAUNCH(true, true, true); else OLB_LAUNCH(true, true, false);
@@ -34,6 +46,22 @@ static cudaError_t launch_step_kind(const StepLaunch& a, bool odd, bool masked, 
   }
 #undef OLB_LAUNCH
   return cudaGetLastError();
+}
+
+template <int Q, class S, class R, int KIND>
+static cudaError_t launch_step_kind(const StepLaunch& a, bool odd, bool masked, bool stats)
+{
+#define OLB_VARIANT(V)                                                                             \
+  launch_step_variant<Q, S, R, KIND, kStepVariants[V].cells_per_thread, kStepVariants[V].min_blocks>( \
+    a, odd, masked, stats)
+  switch (a.variant) {
+  case 0: return OLB_VARIANT(0);
+  case 1: return OLB_VARIANT(1);
+  case 2: return OLB_VARIANT(2);
+  case 3: return OLB_VARIANT(3);
+  default: return cudaErrorInvalidValue;
+  }
+#undef OLB_VARIANT
 }
 
 template <int Q, class S, class R>
@@ -64,11 +92,10 @@ template <int Q, class S, class R>
 cudaError_t launch_scatter(void* pops, const Geometry& g, const void* in, int i_begin, int i_end,
                            cudaStream_t stream)
 {
-  const size_t cells = size_t(g.nx) * g.ny * g.nz;
-  const unsigned threads = 256;
-  const unsigned blocks = unsigned((cells + threads - 1) / threads);
-  scatter_natural_kernel<Q, S, R><<<blocks, threads, 0, stream>>>(static_cast<S*>(pops), g,
-                                                                  static_cast<const R*>(in), i_begin, i_end);
+  const dim3 block(32, 8);
+  const dim3 grid = cell_grid(g, 32, 8);
+  scatter_natural_kernel<Q, S, R><<<grid, block, 0, stream>>>(static_cast<S*>(pops), g,
+                                                              static_cast<const R*>(in), i_begin, i_end);
   return cudaGetLastError();
 }
 

@@ -118,7 +118,9 @@ extern "C" olb_b200_status olb_b200_collide_and_stream_noalloc(
   // the library's default launch shape
   const int bz = desc->nz >= 128 ? 128 : (desc->nz >= 64 ? 64 : 32);
   const int by = 256 / bz;
-  const dim3 grid = step_grid(g, bz, by);
+  // one cell per thread (step variant 0): 65536 blocks cover 256^3 cells
+  const int variant = 0;
+  const dim3 grid = step_grid(g, bz, by, kStepVariants[variant].cells_per_thread);
   const size_t blocks = size_t(grid.x) * grid.y * grid.z;
   if (stats && blocks > kMaxBlocks) {
     char buf[256];
@@ -154,6 +156,7 @@ extern "C" olb_b200_status olb_b200_collide_and_stream_noalloc(
     a.partials = last_stats ? scratch : nullptr;
     a.block_z = bz;
     a.block_y = by;
+    a.variant = variant;
     a.stream = s;
     const bool odd = ((steps_done + k) & 1) != 0;
     switch (desc->storage) {

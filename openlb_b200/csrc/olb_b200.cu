@@ -190,6 +190,9 @@ struct olb_b200_lattice {
   StatPartial* stat_dev = nullptr;
   StatPartial* stat_host = nullptr;  // pinned
   int block_z = 0, block_y = 0;
+  int variant = 0;          // index into kStepVariants
+  bool tuned = false;       // variant and shape chosen by olb_b200_autotune
+  float tuned_ms = 0.f;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   size_t device_bytes = 0;
@@ -209,6 +212,21 @@ void default_shape(const olb_b200_lattice* L, int& bz, int& by)
   bz = L->desc.nz >= 128 ? 128 : (L->desc.nz >= 64 ? 64 : 32);
   by = 256 / bz;
 }
+
+// Default step variant per lattice class, from a 256^3 sweep on B200 (the
+// autotuner refines it on the actual lattice): masked lattices and 16-bit
+// storage keep one cell per thread at high occupancy; FP64 and unmasked
+// FP32 lattices issue the loads of two cells per thread.
+int default_variant(const olb_b200_lattice* L)
+{
+  const int storage = L->desc.storage;
+  if (storage == OLB_B200_STORAGE_F16 || storage == OLB_B200_STORAGE_BF16) return 1;  // {1,4}
+  if (L->masked) return storage == OLB_B200_STORAGE_F64 ? 0 : 1;                  // {1,3} / {1,4}
+  if (storage == OLB_B200_STORAGE_F64) return 2;                                     // {2,2}
+  return 3;                                                                          // {2,3}
+}
+
+int cells_per_thread(const olb_b200_lattice* L) { return kStepVariants[L->variant].cells_per_thread; }
 
 template <class F>
 cudaError_t dispatch(const olb_b200_lattice* L, F&& f)
@@ -232,7 +250,7 @@ cudaError_t dispatch(const olb_b200_lattice* L, F&& f)
 
 olb_b200_status ensure_partials(olb_b200_lattice* L)
 {
-  const dim3 grid = step_grid(L->g, L->block_z, L->block_y);
+  const dim3 grid = step_grid(L->g, L->block_z, L->block_y, cells_per_thread(L));
   const size_t need = size_t(grid.x) * grid.y * grid.z;
   if (need > L->n_partials) {
     if (L->partials) cudaFree(L->partials);
@@ -257,6 +275,7 @@ olb_b200_status enqueue_steps(olb_b200_lattice* L, int steps, bool stats_last)
     a.partials = stats ? L->partials : nullptr;
     a.block_z = L->block_z;
     a.block_y = L->block_y;
+    a.variant = L->variant;
     a.stream = L->stream;
     const bool odd = L->parity == 1;
     cudaError_t e = dispatch(L, [&](auto qc, auto s_, auto r_) {
@@ -305,7 +324,12 @@ olb_b200_status olb_b200_create(const olb_b200_desc* desc, olb_b200_lattice** ou
     return fail(OLB_B200_ERR_ARG, "create: reserved fields must be zero");
   const size_t cells = size_t(desc->nx) * desc->ny * desc->nz;
   if (cells > (size_t(1) << 31)) return fail(OLB_B200_ERR_ARG, "create: %zu cells exceed 2^31", cells);
-  const size_t stride = (cells + 63) / 64 * 64;
+  if (desc->nx > 65535) return fail(OLB_B200_ERR_ARG, "create: nx %d exceeds 65535", desc->nx);
+  // 16-bit storage with an even nx uses the paired layout (two cells per
+  // 4-byte element); its element columns start on 256-byte boundaries too
+  const bool paired = (desc->storage == OLB_B200_STORAGE_F16 || desc->storage == OLB_B200_STORAGE_BF16) &&
+                      desc->nx % 2 == 0;
+  const size_t stride = paired ? (cells + 127) / 128 * 128 : (cells + 63) / 64 * 64;
   if (stride * size_t(desc->q) > (size_t(1) << 40)) return fail(OLB_B200_ERR_ARG, "create: lattice too large");
 
   auto* L = new olb_b200_lattice;
@@ -316,7 +340,7 @@ olb_b200_status olb_b200_create(const olb_b200_desc* desc, olb_b200_lattice** ou
   L->device = desc->device;
   L->elem = desc->storage == OLB_B200_STORAGE_F64 ? 8 : (desc->storage == OLB_B200_STORAGE_F32 ? 4 : 2);
   L->real = desc->storage == OLB_B200_STORAGE_F64 ? 8 : 4;
-  L->g = Geometry{desc->nx, desc->ny, desc->nz, uint32_t(stride)};
+  L->g = Geometry{desc->nx, desc->ny, desc->nz, uint32_t(stride), paired ? 1 : 0};
   default_shape(L, L->block_z, L->block_y);
 
   auto cleanup = [&](olb_b200_status st) {
@@ -435,11 +459,17 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
   std::memcpy(L->bulk, host.data() + bulk_entry * esz, esz);
   // the unmasked kernel serves lattices where every cell uses one fluid entry
   const int only = ids ? first : 0;
+  const bool was_masked = L->masked;
   L->masked = !(uniform && is_fluid(table[only].kind));
   if (!L->masked) {
     std::memcpy(L->bulk, host.data() + only * esz, esz);
   }
   L->n_entries = n_entries;
+  // a change of kernel class invalidates an earlier tuning
+  if (!L->tuned || was_masked != L->masked) {
+    L->variant = default_variant(L);
+    L->tuned = false;
+  }
   return OLB_B200_OK;
 }
 
@@ -521,7 +551,7 @@ olb_b200_status olb_b200_collide_and_stream(olb_b200_lattice* L, int32_t steps, 
   st = enqueue_steps(L, steps, stats != nullptr);
   if (st != OLB_B200_OK) return st;
   if (!stats) return OLB_B200_OK;
-  const dim3 grid = step_grid(L->g, L->block_z, L->block_y);
+  const dim3 grid = step_grid(L->g, L->block_z, L->block_y, cells_per_thread(L));
   const size_t count = size_t(grid.x) * grid.y * grid.z;
   reduce_partials_kernel<<<1, 1024, 0, L->stream>>>(L->partials, count, L->stat_dev);
   OLB_CUDA(cudaGetLastError());
@@ -620,6 +650,109 @@ olb_b200_status olb_b200_set_launch_shape(olb_b200_lattice* L, int32_t block_z, 
                 "of 32, block_z*block_y <= %d", block_z, block_y, kStepThreads);
   L->block_z = block_z;
   L->block_y = block_y;
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_set_step_variant(olb_b200_lattice* L, int32_t variant)
+{
+  g_last_error.clear();
+  if (!L) return fail(OLB_B200_ERR_ARG, "set_step_variant: null lattice");
+  if (variant < -1 || variant >= kNumStepVariants)
+    return fail(OLB_B200_ERR_ARG, "set_step_variant: variant %d outside [-1, %d)", variant, kNumStepVariants);
+  L->variant = variant < 0 ? default_variant(L) : variant;
+  L->tuned = false;
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_get_tuning(olb_b200_lattice* L, olb_b200_tuning* out)
+{
+  if (!L || !out) return fail(OLB_B200_ERR_ARG, "get_tuning: null argument");
+  out->variant = L->variant;
+  out->cells_per_thread = kStepVariants[L->variant].cells_per_thread;
+  out->min_blocks_per_sm = kStepVariants[L->variant].min_blocks;
+  out->block_z = L->block_z;
+  out->block_y = L->block_y;
+  out->tuned = L->tuned ? 1 : 0;
+  out->candidates = 0;
+  out->ms_per_step = L->tuned ? L->tuned_ms : 0.f;
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_autotune(olb_b200_lattice* L, int32_t trial_steps, olb_b200_tuning* out)
+{
+  g_last_error.clear();
+  if (!L) return fail(OLB_B200_ERR_ARG, "autotune: null lattice");
+  if (trial_steps < 0) return fail(OLB_B200_ERR_ARG, "autotune: negative trial steps");
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  const int trials = trial_steps == 0 ? 4 : (trial_steps + 1) / 2 * 2;  // even: same layout parity
+  // the trials advance the state; keep a device copy and restore it afterwards
+  const size_t pop_bytes = L->stride * size_t(L->q) * L->elem;
+  void* backup = nullptr;
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  OLB_CUDA(cudaMalloc(&backup, pop_bytes));
+  cudaError_t e = cudaMemcpyAsync(backup, L->pops, pop_bytes, cudaMemcpyDeviceToDevice, L->stream);
+  if (e != cudaSuccess) {
+    cudaFree(backup);
+    return cuda_fail(e, "autotune backup copy");
+  }
+  const int parity = L->parity;
+  const int64_t steps_done = L->steps_done;
+  const int zmax = std::max(32, (L->desc.nz + 31) / 32 * 32);
+  float best = 0.f;
+  int best_v = L->variant, best_bz = L->block_z, best_by = L->block_y, tried = 0;
+  for (int v = 0; v < kNumStepVariants && st == OLB_B200_OK; ++v) {
+    bool duplicate = false;
+    for (int w = 0; w < v; ++w) {
+      duplicate |= kStepVariants[w].cells_per_thread == kStepVariants[v].cells_per_thread &&
+                   kStepVariants[w].min_blocks == kStepVariants[v].min_blocks;
+    }
+    if (duplicate) continue;
+    for (int bz = 256; bz >= 32 && st == OLB_B200_OK; bz /= 2) {
+      if (bz > zmax) continue;
+      L->variant = v;
+      L->block_z = bz;
+      L->block_y = kStepThreads / bz;
+      st = enqueue_steps(L, 2, false);  // warm-up
+      if (st != OLB_B200_OK) break;
+      if ((e = cudaEventRecord(L->ev0, L->stream)) != cudaSuccess) { st = cuda_fail(e, "autotune event"); break; }
+      st = enqueue_steps(L, trials, false);
+      if (st != OLB_B200_OK) break;
+      float ms = 0.f;
+      if ((e = cudaEventRecord(L->ev1, L->stream)) != cudaSuccess ||
+          (e = cudaEventSynchronize(L->ev1)) != cudaSuccess ||
+          (e = cudaEventElapsedTime(&ms, L->ev0, L->ev1)) != cudaSuccess) {
+        st = cuda_fail(e, "autotune timing");
+        break;
+      }
+      ms /= float(trials);
+      ++tried;
+      if (tried == 1 || ms < best) {
+        best = ms;
+        best_v = v;
+        best_bz = bz;
+        best_by = kStepThreads / bz;
+      }
+    }
+  }
+  // restore the state whatever happened
+  e = cudaMemcpyAsync(L->pops, backup, pop_bytes, cudaMemcpyDeviceToDevice, L->stream);
+  const cudaError_t e2 = cudaStreamSynchronize(L->stream);
+  cudaFree(backup);
+  L->parity = parity;
+  L->steps_done = steps_done;
+  if (st != OLB_B200_OK) return st;
+  if (e != cudaSuccess) return cuda_fail(e, "autotune restore copy");
+  if (e2 != cudaSuccess) return cuda_fail(e2, "autotune synchronize");
+  L->variant = best_v;
+  L->block_z = best_bz;
+  L->block_y = best_by;
+  L->tuned = true;
+  L->tuned_ms = best;
+  if (out) {
+    olb_b200_get_tuning(L, out);
+    out->candidates = tried;
+  }
   return OLB_B200_OK;
 }
 

@@ -156,6 +156,22 @@ class Lattice:
     def set_launch_shape(self, block_z: int, block_y: int) -> None:
         self._check(self._lib.olb_b200_set_launch_shape(self._h, block_z, block_y))
 
+    def set_step_variant(self, variant: int) -> None:
+        """Select a step-kernel variant (-1: the library's default)."""
+        self._check(self._lib.olb_b200_set_step_variant(self._h, int(variant)))
+
+    def autotune(self, trial_steps: int = 0) -> dict:
+        """Time every (variant, launch shape) on this lattice and keep the
+        fastest; the lattice state is restored afterwards."""
+        t = _abi.Tuning()
+        self._check(self._lib.olb_b200_autotune(self._h, int(trial_steps), ctypes.byref(t)))
+        return t.as_dict()
+
+    def tuning(self) -> dict:
+        t = _abi.Tuning()
+        self._check(self._lib.olb_b200_get_tuning(self._h, ctypes.byref(t)))
+        return t.as_dict()
+
     # -- state --------------------------------------------------------------
     def set_populations(self, pops: np.ndarray) -> None:
         pops = np.ascontiguousarray(pops, dtype=self.dtype).reshape(-1)

@@ -1,0 +1,135 @@
+"""Step-kernel variant sweep and autotuning report.
+
+    python -m openlb_b200.tune [--n 256] [--steps 20] [--repeat 3]
+
+For each lattice class (D3Q19 FP32 periodic, D3Q19 FP32 cavity with walls and
+a lid, D3Q19 FP16/BF16, D3Q19 FP64, D3Q27 FP32/FP16) it times every
+step-kernel variant at every launch shape with CUDA events (best of
+`--repeat` runs of `--steps` steps), then runs the autotuner and prints one
+JSON line per measurement and a markdown summary of the fraction of the
+measured HBM copy bandwidth (MEASURED_PEAKS.json) each one reaches.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+from pathlib import Path
+
+import numpy as np
+
+from . import _abi
+from .lattice import BGKdynamics, BounceBack, BounceBackVelocity, Lattice
+from .workloads import cavity
+
+BYTES = {"f32": 4, "f64": 8, "f16": 2, "bf16": 2}
+CLASSES = [
+    ("D3Q19 f32", 19, "f32", False),
+    ("D3Q19 f32 cavity", 19, "f32", True),
+    ("D3Q19 f16", 19, "f16", False),
+    ("D3Q19 bf16", 19, "bf16", False),
+    ("D3Q19 f64", 19, "f64", False),
+    ("D3Q27 f32", 27, "f32", False),
+    ("D3Q27 f16", 27, "f16", False),
+]
+
+
+def peak_gbs() -> float:
+    p = Path(__file__).resolve().parents[1] / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
+
+
+def make_lattice(q, n, storage, masked):
+    lat = Lattice(q, (n, n, n), (not masked,) * 3, storage=storage)
+    if masked:
+        lat.set_dynamics([BGKdynamics(omega=1.6), BounceBack(), BounceBackVelocity((0.1, 0.0, 0.0))],
+                         cavity((n, n, n)))
+    else:
+        lat.set_dynamics([BGKdynamics(omega=1.6)])
+    return lat
+
+
+def time_config(lat, steps, repeat):
+    lat.collide_and_stream(4)
+    lat.synchronize()
+    return min(lat.time_steps(steps) for _ in range(repeat)) / steps
+
+
+def run_single(args):
+    """One fixed configuration: warm-up, then `--steps` steps (for profilers)."""
+    lat = make_lattice(args.lattice, args.n, args.storage, args.masked)
+    try:
+        lat.set_step_variant(args.variant)
+        bz, by = (int(v) for v in args.shape.split(","))
+        lat.set_launch_shape(bz, by)
+        lat.collide_and_stream(args.warmup)
+        lat.synchronize()
+        ms = lat.time_steps(args.steps)
+        cells = args.n ** 3
+        bpc = 2 * args.lattice * BYTES[args.storage]
+        print(json.dumps({"lattice": args.lattice, "n": args.n, "storage": args.storage, "masked": args.masked,
+                          "tuning": lat.tuning(), "ms_per_step": ms / args.steps,
+                          "mlups": round(cells * args.steps / (ms * 1e-3) / 1e6),
+                          "frac": round(cells * bpc * args.steps / (ms * 1e-3) / 1e9 / peak_gbs(), 3)}))
+    finally:
+        lat.close()
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--repeat", type=int, default=3)
+    ap.add_argument("--single", action="store_true",
+                    help="run one fixed configuration (--lattice/--storage/--masked/--variant/--shape)")
+    ap.add_argument("--lattice", type=int, default=19, choices=[19, 27])
+    ap.add_argument("--storage", default="f32", choices=list(BYTES))
+    ap.add_argument("--masked", action="store_true")
+    ap.add_argument("--variant", type=int, default=-1)
+    ap.add_argument("--shape", default="128,2")
+    ap.add_argument("--warmup", type=int, default=3)
+    args = ap.parse_args(argv)
+    if args.single:
+        return run_single(args)
+    peak = peak_gbs()
+    summary = {}
+    for label, q, storage, masked in CLASSES:
+        lat = make_lattice(q, args.n, storage, masked)
+        cells = args.n ** 3
+        bpc = 2 * q * BYTES[storage]
+        best_fixed = {}
+        try:
+            for variant in range(4):
+                lat.set_step_variant(variant)
+                t = lat.tuning()
+                for bz in (256, 128, 64, 32):
+                    lat.set_launch_shape(bz, 256 // bz)
+                    ms = time_config(lat, args.steps, args.repeat)
+                    frac = cells * bpc / (ms * 1e-3) / 1e9 / peak
+                    rec = {"class": label, "variant": variant, "cells_per_thread": t["cells_per_thread"],
+                           "min_blocks": t["min_blocks_per_sm"], "shape": [bz, 256 // bz],
+                           "mlups": round(cells / (ms * 1e-3) / 1e6), "frac": round(frac, 3)}
+                    print(json.dumps(rec), flush=True)
+                    key = (t["cells_per_thread"], t["min_blocks_per_sm"])
+                    best_fixed[key] = max(best_fixed.get(key, 0.0), frac)
+            tuned = lat.autotune(4)
+            ms = time_config(lat, args.steps, args.repeat)
+            frac = cells * bpc / (ms * 1e-3) / 1e9 / peak
+            print(json.dumps({"class": label, "autotuned": tuned, "mlups": round(cells / (ms * 1e-3) / 1e6),
+                              "frac": round(frac, 3)}), flush=True)
+            summary[label] = (best_fixed, tuned, frac, cells / (ms * 1e-3) / 1e6)
+        finally:
+            lat.close()
+    keys = sorted({k for v in summary.values() for k in v[0]})
+    print(f"\n| class | " + " | ".join(f"C{c},B{b}" for c, b in keys) + " | autotuned (C,B,shape) | autotuned GLUPS |")
+    print("|---|" + "---|" * (len(keys) + 2))
+    for label, (best, tuned, frac, mlups) in summary.items():
+        cells = " | ".join(f"{best.get(k, float('nan')):.3f}" for k in keys)
+        print(f"| {label} | {cells} | {tuned['cells_per_thread']},{tuned['min_blocks_per_sm']},"
+              f"({tuned['block_z']},{tuned['block_y']}) {frac:.3f} | {mlups / 1e3:.1f} |")
+
+
+if __name__ == "__main__":
+    main()

@@ -243,3 +243,124 @@ def test_launch_shapes_agree(shape):
     ref, _ = run_oracle(case, f0, 6)
     rel, _ = C.pop_tolerance_violation(19, got, ref, RTOL["f32"])
     assert rel <= RTOL["f32"]
+
+
+@pytest.mark.parametrize("storage", ["f32", "f64", "f16"])
+@pytest.mark.parametrize("masked", [False, True])
+@pytest.mark.parametrize("build", ["exact", "fast"])
+def test_step_variants_agree(storage, masked, build):
+    """Kernel variants differ only in work distribution.  Without FMA
+    contraction (exact build) their results are bit-identical; with it, nvcc
+    may contract differently per instantiation, so the fast build's variants
+    agree to the FP32 parity tolerance."""
+    rng = np.random.default_rng(8)
+    size = (10, 21, 40)
+    case = C.cavity_case(19, size) if masked else C.periodic_case(19, size)
+    dtype = np.float64 if storage == "f64" else np.float32
+    f0 = C.random_state(19, case.n, dtype, rng, amp_u=0.01, amp_neq=1e-4)
+    results = []
+    for variant in range(4):
+        lat = ob.Lattice(19, case.size, case.periodic, storage=storage, variant=build)
+        try:
+            lat.set_dynamics(C.to_abi_table(case), case.dyn_id)
+            lat.set_step_variant(variant)
+            assert lat.tuning()["variant"] == variant
+            lat.set_populations(f0)
+            lat.collide_and_stream(5)
+            results.append(lat.get_populations())
+        finally:
+            lat.close()
+    for r in results[1:]:
+        if build == "exact":
+            assert np.array_equal(r, results[0])
+        elif storage == "f16":
+            # a one-ulp FP32 difference can move a value across a half-precision
+            # rounding boundary: bound by one unit roundoff of the stored value
+            assert np.all(np.abs(r - results[0]) <= 2.0 ** -11 * np.abs(results[0]) + 1e-7)
+        else:
+            rel, _ = C.pop_tolerance_violation(19, r, results[0], RTOL["f32"])
+            assert rel <= RTOL["f32"], rel
+
+
+def test_autotune_restores_state_and_picks_a_candidate():
+    rng = np.random.default_rng(9)
+    case = C.periodic_case(19, (24, 20, 64))
+    f0 = C.random_state(19, case.n, np.float32, rng)
+    lat = ob.Lattice(19, case.size, case.periodic)
+    try:
+        lat.set_dynamics(C.to_abi_table(case))
+        lat.set_populations(f0)
+        lat.collide_and_stream(3)
+        before = lat.get_populations()
+        steps_before = lat.info()["steps_done"]
+        t = lat.autotune(4)
+        assert t["tuned"] == 1 and t["candidates"] >= 4 and t["ms_per_step"] > 0
+        assert lat.info()["steps_done"] == steps_before
+        assert np.array_equal(lat.get_populations(), before)
+        lat.collide_and_stream(2)
+        got = lat.get_populations()
+    finally:
+        lat.close()
+    ref, _ = run_oracle(case, f0, 5)
+    rel, _ = C.pop_tolerance_violation(19, got, ref, RTOL["f32"])
+    assert rel <= RTOL["f32"]
+
+
+def _shear_wave_state(size, dtype, u0=0.04):
+    """Velocity varying along all three axes, so populations cross every face."""
+    nx, ny, nz = size
+    X, Y, Z = np.meshgrid(*(2 * np.pi * (np.arange(s) + 0.5) / s for s in size), indexing="ij")
+    u = np.stack([u0 * np.sin(Y) * np.cos(Z), u0 * np.sin(X) * np.cos(Z), u0 * np.cos(X) * np.sin(Y)])
+    rho = 1 + 0.01 * np.cos(X + Y + Z)
+    n = nx * ny * nz
+    return O.equilibrium(19, rho.reshape(-1).astype(dtype), u.reshape(3, n).astype(dtype))
+
+
+@pytest.mark.parametrize("nx", [2, 4, 6, 5, 24])
+@pytest.mark.parametrize("storage,bound", [("f16", 1e-3), ("bf16", 5e-3)])
+def test_16bit_paired_layout_across_the_x_seam(nx, storage, bound):
+    """16-bit storage pairs cells x and x+nx/2 (even nx); odd nx keeps the
+    natural layout.  Flow crossing the x seam must match the FP64 oracle."""
+    size = (nx, 12, 34)
+    case = C.periodic_case(19, size, omega=1.2)
+    f64 = _shear_wave_state(size, np.float64)
+    ref, _ = run_oracle(case, f64, 20)
+    _, r_u = O.moments(case, ref)
+    got, _, gu, _ = run_gpu(case, f64.astype(np.float32), 20, storage=storage)
+    err = np.linalg.norm(gu - r_u) / np.linalg.norm(r_u)
+    assert err <= bound, err
+    # the populations themselves, relative to the unshifted value
+    rel, _ = C.pop_tolerance_violation(19, got, ref, 1.0)
+    assert rel <= (2e-4 if storage == "f16" else 2e-3), rel
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_16bit_cavity_with_walls(storage):
+    case = C.cavity_case(19, (16, 14, 12))
+    ref64, _ = run_oracle(case, C.rest_state(19, case.n, np.float64), 60)
+    valid = ~np.isnan(ref64)
+    _, r_u = O.moments(case, np.where(valid, ref64, 0))
+    _, _, gu, _ = run_gpu(case, C.rest_state(19, case.n, np.float32), 60, storage=storage)
+    fluid = case.dyn_id == 0
+    err = np.linalg.norm(gu[:, fluid] - r_u[:, fluid]) / np.linalg.norm(r_u[:, fluid])
+    assert err <= (2e-3 if storage == "f16" else 1e-2), err
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+@pytest.mark.parametrize("nx", [8, 7])
+def test_16bit_round_trip(storage, nx):
+    rng = np.random.default_rng(12)
+    q, size = 19, (nx, 6, 5)
+    n = nx * 30
+    f = C.random_state(q, n, np.float32, rng)
+    lat = ob.Lattice(q, size, (True, True, True), storage=storage)
+    try:
+        lat.set_populations(f)
+        back = lat.get_populations()
+    finally:
+        lat.close()
+    # round to nearest in the 16-bit format: at most one unit roundoff of the
+    # stored (shifted, power-of-two scaled) value — 2^-11 for FP16, 2^-8 for
+    # BF16 — plus half the FP16 subnormal spacing for values near zero
+    u = 2.0 ** -11 if storage == "f16" else 2.0 ** -8
+    assert np.all(np.abs(back - f) <= u * np.abs(f) + 2.0 ** -25)

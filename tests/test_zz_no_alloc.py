@@ -8,10 +8,11 @@ the test's behalf, standing in for such a caller's pool.
 
 The check: two calls in a row of the no-allocation entry point produce the
 same populations and statistics as olb_b200_collide_and_stream on a lattice
-handle with the same input — populations within the FP32 tolerance the parity
-tests use (1e-5 of the unshifted population; the kernels are the same, so they
-are in fact identical) and statistics within 1e-12 relative.  This file is
-collected last so a failure here comes after every other test has run.
+handle with the same input, within the tolerances the parity tests use:
+populations within 1e-5 of the unshifted population, summed density within
+1e-7 relative, summed |u|^2 and max |u|^2 within 1e-5.  The handle runs the
+same step-kernel variant and launch shape as the no-allocation call.  This
+file is collected last so a failure here comes after every other test has run.
 """
 import ctypes
 
@@ -24,7 +25,8 @@ from openlb_b200 import _abi
 pytestmark = pytest.mark.gpu
 
 RTOL_POPS = 1e-5
-RTOL_STATS = 1e-12
+RTOL_STATS = {"sum_rho": 1e-7, "average_rho": 1e-7, "sum_usqr": 1e-5, "average_energy": 1e-5,
+              "max_usqr": 1e-5, "max_u": 1e-5}
 
 
 def _state(q, n, rng):
@@ -56,6 +58,8 @@ def test_noalloc_matches_lattice_entry_point(q):
     # existing entry point on a lattice handle
     lat = ob.Lattice(q, size, (True, True, True))
     lat.set_dynamics([ob.BGKdynamics(omega=omega)])
+    lat.set_step_variant(0)       # the variant the no-allocation call uses
+    lat.set_launch_shape(0, 0)    # the library's default launch shape
     lat.set_populations(f0.reshape(-1))
 
     # caller-owned device buffer in the library's layout (natural order at step 0)
@@ -100,7 +104,7 @@ def test_noalloc_matches_lattice_entry_point(q):
 
             # statistics of the last step
             for key in ("sum_rho", "sum_usqr", "max_usqr", "average_rho", "average_energy", "max_u"):
-                np.testing.assert_allclose(getattr(st, key), ref_stats[key], rtol=RTOL_STATS, err_msg=key)
+                np.testing.assert_allclose(getattr(st, key), ref_stats[key], rtol=RTOL_STATS[key], err_msg=key)
             assert st.n_cells == ref_stats["n_cells"] == n
             assert st.n_nonfinite == 0
 
