@@ -219,6 +219,71 @@ olb_b200_status olb_b200_collide_and_stream_noalloc(const olb_b200_desc* desc, v
                                                     const olb_b200_dyn_params* bulk, int32_t steps,
                                                     olb_b200_stats* stats, void* stream);
 
+/* Velocity-change residual ||u - u_prev||_2 / ||u||_2 over the fluid cells,
+ * u_prev being the velocity at the previous call (0 before the first), as the
+ * steady-state criterion of a converging solve; the velocity is kept on the
+ * device.  The reference tracks convergence on the host with
+ * util::ValueTracer over the average energy (src/utilities/benchmarkUtil.h:49-79);
+ * this is the residual the ensemble server below uses as well.  Synchronous. */
+olb_b200_status olb_b200_velocity_residual(olb_b200_lattice* lattice, double* residual);
+
+/* ------------------------------------------------------------------------
+ * Ensemble of independent lattices (the serving layer's device side).  No
+ * counterpart in the reference, which runs one SuperLattice per program.
+ * Instances of different sizes share one device pool and advance together in
+ * one kernel launch per step over a flattened cell index; a chunk of steps is
+ * a replayed CUDA graph.  Instances are admitted while slots and pool memory
+ * last and leave when the host removes them.
+ * ------------------------------------------------------------------------ */
+typedef struct olb_b200_ensemble olb_b200_ensemble;
+
+typedef enum {
+  OLB_B200_ENSEMBLE_CAVITY = 1,   /* lid-driven cavity: bounce-back box, lid wall_u on y = ny-1,
+                                     BGK fluid (cavity3dBenchmark geometry) */
+  OLB_B200_ENSEMBLE_CHANNEL = 2   /* x-periodic channel, bounce-back walls at y and z faces,
+                                     Guo-forced BGK fluid with body force `force` */
+} olb_b200_instance_kind;
+
+typedef struct {
+  int32_t q;              /* 19 */
+  int32_t storage;        /* OLB_B200_STORAGE_F32 */
+  int32_t device;
+  int32_t max_instances;  /* slots */
+  uint64_t pool_bytes;    /* device memory for all instances (admission budget) */
+} olb_b200_ensemble_desc;
+
+typedef struct {
+  int32_t kind;           /* olb_b200_instance_kind */
+  int32_t nx, ny, nz;
+  double omega;
+  double wall_u[3];       /* lid velocity (cavity) */
+  double force[3];        /* body force (channel) */
+} olb_b200_instance_desc;
+
+olb_b200_status olb_b200_ensemble_create(const olb_b200_ensemble_desc* desc, olb_b200_ensemble** out);
+void olb_b200_ensemble_destroy(olb_b200_ensemble* ensemble);
+/* Admits an instance at rest (rho = 1, u = 0); OLB_B200_ERR_OOM when no slot
+ * or not enough pool memory is free (the caller queues the request). */
+olb_b200_status olb_b200_ensemble_add(olb_b200_ensemble* ensemble, const olb_b200_instance_desc* desc,
+                                      int32_t* slot);
+olb_b200_status olb_b200_ensemble_remove(olb_b200_ensemble* ensemble, int32_t slot);
+/* Advances every active instance by `steps` steps.  With check != 0 a pass
+ * after the last step computes each instance's velocity-change residual
+ * against the previous check (as olb_b200_velocity_residual does).
+ * residual / steps_done (max_instances entries each, may be NULL) receive the
+ * per-slot values.  Synchronous. */
+olb_b200_status olb_b200_ensemble_run(olb_b200_ensemble* ensemble, int32_t steps, int32_t check,
+                                      double* residual, uint32_t* steps_done);
+/* Density / velocity of one instance (n and 3n floats, z fastest). */
+olb_b200_status olb_b200_ensemble_get_moments(olb_b200_ensemble* ensemble, int32_t slot, float* rho, float* u);
+olb_b200_status olb_b200_ensemble_info(olb_b200_ensemble* ensemble, int64_t* pool_free_bytes,
+                                       int32_t* active, int32_t* tiles);
+/* Resident blocks per SM of the batched kernel (2, 3 or 4); the grid is that
+ * many blocks per SM. */
+olb_b200_status olb_b200_ensemble_set_occupancy(olb_b200_ensemble* ensemble, int32_t blocks_per_sm);
+/* Pool bytes one instance of this extent occupies. */
+uint64_t olb_b200_ensemble_bytes_per_instance(int32_t nx, int32_t ny, int32_t nz);
+
 /* Thread-local message of the last failed call on this thread ("" if none). */
 const char* olb_b200_last_error(void);
 

@@ -38,8 +38,13 @@ EXPORTED = [
     "olb_b200_synchronize", "olb_b200_time_steps", "olb_b200_get_stream", "olb_b200_get_info",
     "olb_b200_set_launch_shape", "olb_b200_last_error", "olb_b200_abi_version",
     "olb_b200_build_info", "olb_b200_collide_and_stream_noalloc", "olb_b200_autotune",
-    "olb_b200_get_tuning", "olb_b200_set_step_variant",
+    "olb_b200_get_tuning", "olb_b200_set_step_variant", "olb_b200_velocity_residual",
+    "olb_b200_ensemble_create", "olb_b200_ensemble_destroy", "olb_b200_ensemble_add",
+    "olb_b200_ensemble_remove", "olb_b200_ensemble_run", "olb_b200_ensemble_get_moments",
+    "olb_b200_ensemble_info", "olb_b200_ensemble_set_occupancy", "olb_b200_ensemble_bytes_per_instance",
 ]
+
+ENSEMBLE_CAVITY, ENSEMBLE_CHANNEL = 1, 2
 
 
 class LibraryNotBuilt(RuntimeError):
@@ -90,6 +95,17 @@ class Tuning(ctypes.Structure):
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class EnsembleDesc(ctypes.Structure):
+    _fields_ = [("q", ctypes.c_int32), ("storage", ctypes.c_int32), ("device", ctypes.c_int32),
+                ("max_instances", ctypes.c_int32), ("pool_bytes", ctypes.c_uint64)]
+
+
+class InstanceDesc(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
+                ("nz", ctypes.c_int32), ("omega", ctypes.c_double), ("wall_u", ctypes.c_double * 3),
+                ("force", ctypes.c_double * 3)]
 
 
 _loaded: dict = {}
@@ -151,6 +167,27 @@ def load(variant: str = "fast") -> ctypes.CDLL:
     lib.olb_b200_get_tuning.restype = st
     lib.olb_b200_set_step_variant.argtypes = [P, ctypes.c_int32]
     lib.olb_b200_set_step_variant.restype = st
+    lib.olb_b200_velocity_residual.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+    lib.olb_b200_velocity_residual.restype = st
+    lib.olb_b200_ensemble_create.argtypes = [ctypes.POINTER(EnsembleDesc), ctypes.POINTER(P)]
+    lib.olb_b200_ensemble_create.restype = st
+    lib.olb_b200_ensemble_destroy.argtypes = [P]
+    lib.olb_b200_ensemble_destroy.restype = None
+    lib.olb_b200_ensemble_add.argtypes = [P, ctypes.POINTER(InstanceDesc), ctypes.POINTER(ctypes.c_int32)]
+    lib.olb_b200_ensemble_add.restype = st
+    lib.olb_b200_ensemble_remove.argtypes = [P, ctypes.c_int32]
+    lib.olb_b200_ensemble_remove.restype = st
+    lib.olb_b200_ensemble_run.argtypes = [P, ctypes.c_int32, ctypes.c_int32, P, P]
+    lib.olb_b200_ensemble_run.restype = st
+    lib.olb_b200_ensemble_get_moments.argtypes = [P, ctypes.c_int32, P, P]
+    lib.olb_b200_ensemble_get_moments.restype = st
+    lib.olb_b200_ensemble_info.argtypes = [P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.POINTER(ctypes.c_int32)]
+    lib.olb_b200_ensemble_info.restype = st
+    lib.olb_b200_ensemble_set_occupancy.argtypes = [P, ctypes.c_int32]
+    lib.olb_b200_ensemble_set_occupancy.restype = st
+    lib.olb_b200_ensemble_bytes_per_instance.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
+    lib.olb_b200_ensemble_bytes_per_instance.restype = ctypes.c_uint64
     lib.olb_b200_last_error.argtypes = []
     lib.olb_b200_last_error.restype = ctypes.c_char_p
     lib.olb_b200_abi_version.argtypes = []

@@ -57,6 +57,16 @@ OLB_HD uint32_t cell_slot(const Geometry& g, int x, int y, int z)
 
 OLB_HD int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
+// A copy of v the compiler cannot see through: store addresses computed from
+// it are recomputed after the collision (one multiply-add each) instead of
+// being kept live in registers from the load phase.
+OLB_DEV uint32_t opaque(uint32_t v)
+{
+  uint32_t r;
+  asm volatile("mov.b32 %0, %1;" : "=r"(r) : "r"(v));
+  return r;
+}
+
 // per-block partial of the fused statistics reduction (FP64)
 struct StatPartial {
   double sum_rho;
@@ -280,13 +290,15 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict
     }
     // NoDynamics (and anything else): populations pass through unchanged
     Neighbours nb(g, x, y, z);
+    const uint32_t stride = opaque(g.stride);
+    const uint32_t nk = opaque(n[k]);
     static_for<0, Q>([&](auto i) {
       if constexpr (!ODD) {
         constexpr int o = L::opp(i);
-        ST::template store<L, o>(pops + size_t(o) * g.stride + n[k], f[k][i]);
+        ST::template store<L, o>(pops + size_t(o) * stride + nk, f[k][i]);
       } else {
         const uint32_t dst = nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>();
-        ST::template store<L, i.value>(pops + size_t(i.value) * g.stride + dst, f[k][i]);
+        ST::template store<L, i.value>(pops + size_t(i.value) * stride + dst, f[k][i]);
       }
     });
     if constexpr (STATS) {
@@ -507,10 +519,12 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
     cell(std::integral_constant<bool, false>{}, kind_lo[k], p_lo[k]);
     cell(std::integral_constant<bool, true>{}, kind_hi[k], p_hi[k]);
     PairNeighbours nb(g, xp, y, z);
+    const uint32_t ps = opaque(pstride);
+    const uint32_t ek = opaque(e[k]);
     static_for<0, Q>([&](auto i) {
       if constexpr (!ODD) {
         constexpr int o = L::opp(i);
-        pops[size_t(o) * pstride + e[k]] = raw[k][i];
+        pops[size_t(o) * ps + ek] = raw[k][i];
       } else {
         const uint32_t dst = nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>();
         T v = raw[k][i];
@@ -518,7 +532,7 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
           v.x = raw[k][i].y;
           v.y = raw[k][i].x;
         }
-        pops[size_t(i.value) * pstride + dst] = v;
+        pops[size_t(i.value) * ps + dst] = v;
       }
     });
   });

@@ -153,13 +153,20 @@ OLB_DEV void compute_j(const R (&f)[L::q], R (&j)[3])
   });
 }
 
-// lbm::computeRhoU  src/dynamics/lbm.h:300-307
+// lbm::computeRhoU  src/dynamics/lbm.h:300-307.  The exact build divides each
+// component as the reference does; the fast build multiplies by one
+// reciprocal (within one ulp of the quotient).
 template <class L, class R>
 OLB_DEV void compute_rho_u(const R (&f)[L::q], R& rho, R (&u)[3])
 {
   rho = compute_rho<L>(f);
   compute_j<L>(f, u);
+#ifdef OLB_B200_EXACT
   u[0] /= rho; u[1] /= rho; u[2] /= rho;
+#else
+  const R inv = R(1) / rho;
+  u[0] *= inv; u[1] *= inv; u[2] *= inv;
+#endif
 }
 
 // ForcedMomentum<BulkMomentum>::computeU after BulkDensity
@@ -213,9 +220,9 @@ OLB_DEV R feq2(R rho, const R (&u)[3], R usqr)
 // collisions (in place on f; return the CellStatistic {rho, uSqr})
 
 // collision::BGK  src/dynamics/collision.h:67-78 with equilibria::SecondOrder
-// (src/dynamics/equilibrium.h:160-167)
+// (src/dynamics/equilibrium.h:160-167), in the reference's operation order
 template <class L, class R>
-OLB_DEV void relax_bgk(R (&f)[L::q], R rho, const R (&u)[3], R omega)
+OLB_DEV void relax_bgk_reference(R (&f)[L::q], R rho, const R (&u)[3], R omega)
 {
   const R usqr = norm_sqr(u);
   static_for<0, L::q>([&](auto i) {
@@ -225,9 +232,9 @@ OLB_DEV void relax_bgk(R (&f)[L::q], R rho, const R (&u)[3], R omega)
   });
 }
 
-// collision::TRT  src/dynamics/collision.h:220-245
+// collision::TRT  src/dynamics/collision.h:220-245, reference operation order
 template <class L, class R>
-OLB_DEV void relax_trt(R (&f)[L::q], R rho, const R (&u)[3], R omega, R omega_minus)
+OLB_DEV void relax_trt_reference(R (&f)[L::q], R rho, const R (&u)[3], R omega, R omega_minus)
 {
   const R usqr = norm_sqr(u);
   R fe[L::q];
@@ -242,6 +249,84 @@ OLB_DEV void relax_trt(R (&f)[L::q], R rho, const R (&u)[3], R omega, R omega_mi
     out[i] = f[i] - (omega * (fp - fep) + omega_minus * (fm - fem));
   });
   static_for<0, L::q>([&](auto i) { f[i] = out[i]; });
+}
+
+// The same two collisions evaluated over opposite pairs.  For c_o = -c_i the
+// second-order equilibria share their even part:
+//   feq_i = A + B,  feq_o = A - B,
+//   A = rho t (1 + 9/2 (c.u)^2 - 3/2 |u|^2) - t,   B = 3 rho t (c.u),
+// so each pair costs one c.u, one even and one odd term; products of rho with
+// a weight are shared between directions of the same weight.  Algebraically
+// identical to the reference; rounding differs by a few ulp.
+template <class L, class R>
+OLB_DEV void relax_bgk_paired(R (&f)[L::q], R rho, const R (&u)[3], R omega)
+{
+  const R usqr = norm_sqr(u);
+  const R even0 = R(1) - R(1.5) * usqr;
+  const R keep = R(1) - omega;
+  {
+    constexpr R t = weight<L, R>(0);
+    f[0] = keep * f[0] + omega * (rho * t * even0 - t);
+  }
+  static_for<1, L::half + 1>([&](auto i) {
+    constexpr int o = L::opp(i);
+    constexpr R t = weight<L, R>(i);
+    const R rt = rho * t;
+    const R cu = c_dot<L, i.value>(u);
+    const R a = rt * (even0 + R(4.5) * cu * cu) - t;
+    const R b = (rt * R(3)) * cu;
+    const R fi = keep * f[i] + omega * (a + b);
+    const R fo = keep * f[o] + omega * (a - b);
+    f[i] = fi;
+    f[o] = fo;
+  });
+}
+
+template <class L, class R>
+OLB_DEV void relax_trt_paired(R (&f)[L::q], R rho, const R (&u)[3], R omega, R omega_minus)
+{
+  const R usqr = norm_sqr(u);
+  const R even0 = R(1) - R(1.5) * usqr;
+  {
+    constexpr R t = weight<L, R>(0);
+    f[0] -= omega * (f[0] - (rho * t * even0 - t));
+  }
+  static_for<1, L::half + 1>([&](auto i) {
+    constexpr int o = L::opp(i);
+    constexpr R t = weight<L, R>(i);
+    const R rt = rho * t;
+    const R cu = c_dot<L, i.value>(u);
+    const R a = rt * (even0 + R(4.5) * cu * cu) - t;  // symmetric part of feq
+    const R b = (rt * R(3)) * cu;                      // antisymmetric part
+    const R dp = omega * (R(0.5) * (f[i] + f[o]) - a);
+    const R dm = omega_minus * (R(0.5) * (f[i] - f[o]) - b);
+    const R fi = f[i] - dp - dm;
+    const R fo = f[o] - dp + dm;
+    f[i] = fi;
+    f[o] = fo;
+  });
+}
+
+// The exact (-fmad=false) build keeps the reference's operation order so it
+// reproduces the reference bit for bit; the fast build uses the pair form.
+template <class L, class R>
+OLB_DEV void relax_bgk(R (&f)[L::q], R rho, const R (&u)[3], R omega)
+{
+#ifdef OLB_B200_EXACT
+  relax_bgk_reference<L>(f, rho, u, omega);
+#else
+  relax_bgk_paired<L>(f, rho, u, omega);
+#endif
+}
+
+template <class L, class R>
+OLB_DEV void relax_trt(R (&f)[L::q], R rho, const R (&u)[3], R omega, R omega_minus)
+{
+#ifdef OLB_B200_EXACT
+  relax_trt_reference<L>(f, rho, u, omega, omega_minus);
+#else
+  relax_trt_paired<L>(f, rho, u, omega, omega_minus);
+#endif
 }
 
 // lbm::addExternalForce (Guo)  src/dynamics/lbm.h:544-566

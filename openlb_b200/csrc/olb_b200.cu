@@ -66,6 +66,31 @@ __global__ void reduce_partials_kernel(const StatPartial* __restrict__ parts, si
   }
 }
 
+// velocity-change residual sums over the fluid cells; stores u as u_prev
+template <class R>
+__global__ void velocity_residual_kernel(const R* __restrict__ u_now, R* __restrict__ u_prev,
+                                         const uint8_t* __restrict__ ids,
+                                         const DynDevice<R>* __restrict__ table, size_t cells,
+                                         StatPartial* __restrict__ partials)
+{
+  const size_t n = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+  double du2 = 0., u2 = 0.;
+  if (n < cells) {
+    const int kind = table[ids ? ids[n] : 0].kind;
+    if (kind == K_BGK || kind == K_TRT || kind == K_SMAGORINSKY || kind == K_FORCED_BGK ||
+        kind == K_FORCED_TRT) {
+      for (int d = 0; d < 3; ++d) {
+        const R u = u_now[d * cells + n];
+        const double du = double(u) - double(u_prev[d * cells + n]);
+        du2 += du * du;
+        u2 += double(u) * double(u);
+        u_prev[d * cells + n] = u;
+      }
+    }
+  }
+  block_stats(du2, u2, 0., 0ull, 0ull, partials);
+}
+
 } // namespace olb_b200
 
 using namespace olb_b200;
@@ -187,6 +212,7 @@ struct olb_b200_lattice {
   void* scratch = nullptr;  // staging, 4 * cells * real bytes
   StatPartial* partials = nullptr;
   size_t n_partials = 0;
+  void* uprev = nullptr;    // velocity at the last residual call (3 * cells * real)
   StatPartial* stat_dev = nullptr;
   StatPartial* stat_host = nullptr;  // pinned
   int block_z = 0, block_y = 0;
@@ -248,10 +274,16 @@ cudaError_t dispatch(const olb_b200_lattice* L, F&& f)
   return cudaErrorInvalidValue;
 }
 
+olb_b200_status ensure_partial_count(olb_b200_lattice* L, size_t need);
+
 olb_b200_status ensure_partials(olb_b200_lattice* L)
 {
   const dim3 grid = step_grid(L->g, L->block_z, L->block_y, cells_per_thread(L));
-  const size_t need = size_t(grid.x) * grid.y * grid.z;
+  return ensure_partial_count(L, size_t(grid.x) * grid.y * grid.z);
+}
+
+olb_b200_status ensure_partial_count(olb_b200_lattice* L, size_t need)
+{
   if (need > L->n_partials) {
     if (L->partials) cudaFree(L->partials);
     L->partials = nullptr;
@@ -389,6 +421,7 @@ void olb_b200_destroy(olb_b200_lattice* L)
   if (L->table) cudaFree(L->table);
   if (L->scratch) cudaFree(L->scratch);
   if (L->partials) cudaFree(L->partials);
+  if (L->uprev) cudaFree(L->uprev);
   if (L->stat_dev) cudaFree(L->stat_dev);
   if (L->stat_host) cudaFreeHost(L->stat_host);
   if (L->ev0) cudaEventDestroy(L->ev0);
@@ -650,6 +683,48 @@ olb_b200_status olb_b200_set_launch_shape(olb_b200_lattice* L, int32_t block_z, 
                 "of 32, block_z*block_y <= %d", block_z, block_y, kStepThreads);
   L->block_z = block_z;
   L->block_y = block_y;
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_velocity_residual(olb_b200_lattice* L, double* residual)
+{
+  g_last_error.clear();
+  if (!L || !residual) return fail(OLB_B200_ERR_ARG, "velocity_residual: null argument");
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  const size_t ubytes = 3 * L->cells * L->real;
+  if (!L->uprev) {
+    OLB_CUDA(cudaMalloc(&L->uprev, ubytes));
+    OLB_CUDA(cudaMemsetAsync(L->uprev, 0, ubytes, L->stream));
+    L->device_bytes += ubytes;
+  }
+  char* rho_d = static_cast<char*>(L->scratch);
+  char* u_d = rho_d + L->cells * L->real;
+  cudaError_t e = dispatch(L, [&](auto qc, auto s_, auto r_) {
+    return launch_moments<decltype(qc)::value, decltype(s_), decltype(r_)>(
+      L->pops, L->g, L->parity == 1, L->ids, L->table, rho_d, u_d, L->stream);
+  });
+  if (e != cudaSuccess) return cuda_fail(e, "moments kernel");
+  const unsigned threads = 256;
+  const size_t blocks = (L->cells + threads - 1) / threads;
+  st = ensure_partial_count(L, blocks);
+  if (st != OLB_B200_OK) return st;
+  if (L->real == 8) {
+    velocity_residual_kernel<double><<<unsigned(blocks), threads, 0, L->stream>>>(
+      reinterpret_cast<const double*>(u_d), static_cast<double*>(L->uprev), L->ids,
+      static_cast<const DynDevice<double>*>(L->table), L->cells, L->partials);
+  } else {
+    velocity_residual_kernel<float><<<unsigned(blocks), threads, 0, L->stream>>>(
+      reinterpret_cast<const float*>(u_d), static_cast<float*>(L->uprev), L->ids,
+      static_cast<const DynDevice<float>*>(L->table), L->cells, L->partials);
+  }
+  OLB_CUDA(cudaGetLastError());
+  reduce_partials_kernel<<<1, 1024, 0, L->stream>>>(L->partials, blocks, L->stat_dev);
+  OLB_CUDA(cudaGetLastError());
+  OLB_CUDA(cudaMemcpyAsync(L->stat_host, L->stat_dev, sizeof(StatPartial), cudaMemcpyDeviceToHost, L->stream));
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  const StatPartial p = *L->stat_host;
+  *residual = p.sum_usqr > 0. ? std::sqrt(p.sum_rho / p.sum_usqr) : (p.sum_rho > 0. ? INFINITY : 0.);
   return OLB_B200_OK;
 }
 

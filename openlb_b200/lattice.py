@@ -209,6 +209,12 @@ class Lattice:
     def synchronize(self) -> None:
         self._check(self._lib.olb_b200_synchronize(self._h))
 
+    def velocity_residual(self) -> float:
+        """||u - u_prev|| / ||u|| over fluid cells since the previous call."""
+        r = ctypes.c_double()
+        self._check(self._lib.olb_b200_velocity_residual(self._h, ctypes.byref(r)))
+        return float(r.value)
+
     def time_steps(self, steps: int) -> float:
         ms = ctypes.c_float()
         self._check(self._lib.olb_b200_time_steps(self._h, int(steps), ctypes.byref(ms)))

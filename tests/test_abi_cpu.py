@@ -15,7 +15,7 @@ HEADER = Path(__file__).resolve().parents[1] / "include" / "olb_b200.h"
 
 def declared_functions():
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:olb_b200_status|void|int32_t|const char\*)\s+(olb_b200_\w+)\(",
+    return sorted(set(re.findall(r"^\s*(?:olb_b200_status|void|int32_t|uint64_t|const char\*)\s+(olb_b200_\w+)\(",
                                  text, flags=re.M)))
 
 
