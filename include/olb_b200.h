@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define OLB_B200_ABI_VERSION 1
+#define OLB_B200_ABI_VERSION 2
 
 typedef struct olb_b200_lattice olb_b200_lattice;
 
@@ -67,7 +67,12 @@ typedef enum {
   OLB_B200_DYN_BOUNCE_BACK = 4,          /* BounceBack              src/dynamics/dynamics.h:472-483 */
   OLB_B200_DYN_BOUNCE_BACK_VELOCITY = 5, /* BounceBackVelocity      src/dynamics/dynamics.h:549-555 */
   OLB_B200_DYN_FORCED_BGK = 6,           /* ForcedBGKdynamics       src/dynamics/dynamics.h:214 */
-  OLB_B200_DYN_FORCED_TRT = 7            /* ForcedTRTdynamics       src/dynamics/dynamics.h:457-464 */
+  OLB_B200_DYN_FORCED_TRT = 7,           /* ForcedTRTdynamics       src/dynamics/dynamics.h:457-464 */
+  /* Interpolated boundaries on a flat face (discrete normal type Flat): the
+   * mixin dynamics with exchanged momenta, plus PlaneFdBoundaryProcessor3D in
+   * the PostStream stage (src/boundary/boundaryPostProcessors3D.hh:39-92). */
+  OLB_B200_DYN_INTERPOLATED_VELOCITY = 8, /* boundary::InterpolatedVelocity  src/boundary/interpolatedVelocity3D.h:44-81 */
+  OLB_B200_DYN_INTERPOLATED_PRESSURE = 9  /* boundary::InterpolatedPressure  src/boundary/interpolatedPressure3D.h:47-90 */
 } olb_b200_dyn_kind;
 
 typedef struct {
@@ -86,16 +91,26 @@ typedef struct {
  *   smagorinsky  collision::LES::SMAGORINSKY    (src/dynamics/collisionLES.h:70)
  *   force        descriptors::FORCE field value (Guo forcing, forcing.h:38-74)
  *   wall_u       descriptors::VELOCITY field of BounceBackVelocity (defineU)
- *   wall_rho     FixedDensity RHO field (1 unless defineRho)               */
+ *   wall_rho     FixedDensity RHO field (1 unless defineRho)
+ * Interpolated boundary entries also carry
+ *   mixin        the MixinDynamics template argument of boundary::Interpolated*
+ *                (BGK, TRT or SMAGORINSKY; must be the lattice's fluid collision)
+ *   direction,   the discrete normal of the face as the boundary setter derives
+ *   orientation  it (src/boundary/setBoundary3D.h:204-227): axis 0..2 and the
+ *                sign of the outward normal, -1 or +1.  All cells of one entry
+ *                should lie in one plane: their boundary values are stored over
+ *                the bounding box of the entry's cells. */
 typedef struct {
   int32_t kind;         /* olb_b200_dyn_kind */
-  int32_t reserved;
+  int32_t mixin;        /* olb_b200_dyn_kind of the mixin (interpolated boundaries), else 0 */
   double omega;
   double magic;
   double smagorinsky;
   double force[3];
   double wall_u[3];
   double wall_rho;
+  int32_t direction;    /* interpolated boundaries: normal axis */
+  int32_t orientation;  /* interpolated boundaries: normal sign */
 } olb_b200_dyn_params;
 
 /* Statistics of one step as OpenLB's LatticeStatistics reports them
@@ -128,6 +143,23 @@ void olb_b200_destroy(olb_b200_lattice* lattice);
 olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* lattice, const uint8_t* ids,
                                       const olb_b200_dyn_params* table, int32_t n_entries);
 
+/* Boundary values of interpolated boundary cells — replaces defineRho /
+ * defineU on their cells (src/core/cell.h:194-198; FixedDensity RHO of
+ * pressure cells, the VELOCITY field of FixedVelocityMomentumGeneric /
+ * FixedPressureMomentum).  values[4*j .. 4*j+3] = RHO, VELOCITY x, y, z of
+ * cells[j] (logical cell index).  RHO is unused by velocity cells and the
+ * normal VELOCITY component by pressure cells.  Until set, RHO = 1 and
+ * VELOCITY = 0.  Synchronous. */
+olb_b200_status olb_b200_set_boundary_values(olb_b200_lattice* lattice, const int64_t* cells, int64_t count,
+                                             const double* values);
+
+/* SuperLattice::initialize (src/core/superLattice.hh:191-204,
+ * src/core/blockLattice.hh:56-67): applies the PostStream post-processors
+ * (the interpolated boundaries) once to the current state.  The first
+ * collide_and_stream does it implicitly when it has not been done; later
+ * calls do nothing.  Synchronous. */
+olb_b200_status olb_b200_initialize(olb_b200_lattice* lattice);
+
 /* Full population state, host <-> device — replaces
  * setProcessingContext(Simulation/Evaluation) for POPULATION
  * (src/core/platform/gpu/cuda/column.hh:157-187,285-296).  Logical layout. */
@@ -137,7 +169,9 @@ olb_b200_status olb_b200_get_populations(olb_b200_lattice* lattice, void* host_p
 /* The hot path — replaces SuperLattice::collideAndStream
  * (src/core/superLattice.hh:601-663): collide (gpu/cuda/operator.hh:311-318)
  * fused with streaming (column.h:144-154, blockLattice.hh:317-339) in one
- * kernel per step.  Runs `steps` steps.  With stats == NULL the call only
+ * kernel per step, then the PostStream stage when the lattice has
+ * interpolated boundary cells (two small kernels over those cells).  Runs
+ * `steps` steps.  With stats == NULL the call only
  * enqueues work on the lattice's stream and returns; with stats != NULL the
  * last step also reduces the statistics, the call waits for them and returns
  * OLB_B200_ERR_DIVERGED if any cell was non-finite. */

@@ -4,11 +4,11 @@ The compute path is the in-tree sm_100a library ``libolb_b200.so`` (C ABI in
 ``include/olb_b200.h``); this package binds it and mirrors the reference's
 host-side lattice API.  There is no CPU fallback.
 """
-from . import _abi
+from . import _abi, boundary
 from .descriptors import D3Q19, D3Q27, Descriptor, descriptor
 from .lattice import (BGKdynamics, BounceBack, BounceBackVelocity, Dynamics, ForcedBGKdynamics,
-                      ForcedTRTdynamics, Lattice, NoDynamics, SmagorinskyBGKdynamics, SuperGeometry,
-                      SuperLattice, TRTdynamics)
+                      ForcedTRTdynamics, InterpolatedPressureBoundary, InterpolatedVelocityBoundary, Lattice,
+                      NoDynamics, SmagorinskyBGKdynamics, SuperGeometry, SuperLattice, TRTdynamics)
 
 OlbError = _abi.OlbError
 Diverged = _abi.Diverged
@@ -26,6 +26,7 @@ def build_info() -> str:
 __all__ = [
     "D3Q19", "D3Q27", "Descriptor", "descriptor", "Dynamics", "NoDynamics", "BGKdynamics",
     "TRTdynamics", "ForcedTRTdynamics", "ForcedBGKdynamics", "SmagorinskyBGKdynamics", "BounceBack",
-    "BounceBackVelocity", "Lattice", "SuperGeometry", "SuperLattice", "OlbError", "Diverged",
+    "BounceBackVelocity", "InterpolatedVelocityBoundary", "InterpolatedPressureBoundary", "boundary",
+    "Lattice", "SuperGeometry", "SuperLattice", "OlbError", "Diverged",
     "LibraryNotBuilt", "library_path", "build_info",
 ]

@@ -30,7 +30,9 @@ STORAGE = {"f32": 0, "f64": 1, "f16": 2, "bf16": 3}
 
 # dynamics kinds (olb_b200_dyn_kind)
 DYN_NONE, DYN_BGK, DYN_TRT, DYN_SMAGORINSKY, DYN_BOUNCE_BACK, DYN_BOUNCE_BACK_VELOCITY, \
-    DYN_FORCED_BGK, DYN_FORCED_TRT = range(8)
+    DYN_FORCED_BGK, DYN_FORCED_TRT, DYN_INTERPOLATED_VELOCITY, DYN_INTERPOLATED_PRESSURE = range(10)
+DYN_INTERPOLATED = (DYN_INTERPOLATED_VELOCITY, DYN_INTERPOLATED_PRESSURE)
+ABI_VERSION = 2
 
 EXPORTED = [
     "olb_b200_create", "olb_b200_destroy", "olb_b200_set_dynamics", "olb_b200_set_populations",
@@ -42,6 +44,7 @@ EXPORTED = [
     "olb_b200_ensemble_create", "olb_b200_ensemble_destroy", "olb_b200_ensemble_add",
     "olb_b200_ensemble_remove", "olb_b200_ensemble_run", "olb_b200_ensemble_get_moments",
     "olb_b200_ensemble_info", "olb_b200_ensemble_set_occupancy", "olb_b200_ensemble_bytes_per_instance",
+    "olb_b200_set_boundary_values", "olb_b200_initialize",
 ]
 
 ENSEMBLE_CAVITY, ENSEMBLE_CHANNEL = 1, 2
@@ -71,10 +74,11 @@ class Desc(ctypes.Structure):
 
 
 class DynParams(ctypes.Structure):
-    _fields_ = [("kind", ctypes.c_int32), ("reserved", ctypes.c_int32),
+    _fields_ = [("kind", ctypes.c_int32), ("mixin", ctypes.c_int32),
                 ("omega", ctypes.c_double), ("magic", ctypes.c_double),
                 ("smagorinsky", ctypes.c_double), ("force", ctypes.c_double * 3),
-                ("wall_u", ctypes.c_double * 3), ("wall_rho", ctypes.c_double)]
+                ("wall_u", ctypes.c_double * 3), ("wall_rho", ctypes.c_double),
+                ("direction", ctypes.c_int32), ("orientation", ctypes.c_int32)]
 
 
 class Stats(ctypes.Structure):
@@ -188,6 +192,10 @@ def load(variant: str = "fast") -> ctypes.CDLL:
     lib.olb_b200_ensemble_set_occupancy.restype = st
     lib.olb_b200_ensemble_bytes_per_instance.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]
     lib.olb_b200_ensemble_bytes_per_instance.restype = ctypes.c_uint64
+    lib.olb_b200_set_boundary_values.argtypes = [P, P, ctypes.c_int64, P]
+    lib.olb_b200_set_boundary_values.restype = st
+    lib.olb_b200_initialize.argtypes = [P]
+    lib.olb_b200_initialize.restype = st
     lib.olb_b200_last_error.argtypes = []
     lib.olb_b200_last_error.restype = ctypes.c_char_p
     lib.olb_b200_abi_version.argtypes = []

@@ -287,6 +287,11 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict
       const R wu[3] = {__ldg(&e->wall_u[0]), __ldg(&e->wall_u[1]), __ldg(&e->wall_u[2])};
       st_usqr = norm_sqr(wu);
       counted = true;
+    } else if (MASKED && is_interpolated(kind[k])) {
+      if constexpr (KIND == K_BGK || KIND == K_TRT || KIND == K_SMAGORINSKY) {
+        collide_interpolated<L, KIND>(f[k], kind[k], p[k], x, y, z, st_rho, st_usqr);
+        counted = true;
+      }
     }
     // NoDynamics (and anything else): populations pass through unchanged
     Neighbours nb(g, x, y, z);
@@ -368,7 +373,7 @@ struct PairNeighbours {
 // collision of one cell of a pair by its runtime kind (masked lattices)
 template <class L, int KIND, bool MASKED>
 OLB_DEV bool collide_any(float (&f)[L::q], int kind, const DynDevice<float>* e, const DynDevice<float>& bulk,
-                         float& st_rho, float& st_usqr)
+                         int x, int y, int z, float& st_rho, float& st_usqr)
 {
   if (kind == KIND) {
     if constexpr (MASKED) {
@@ -401,6 +406,11 @@ OLB_DEV bool collide_any(float (&f)[L::q], int kind, const DynDevice<float>* e, 
       const float wu[3] = {__ldg(&e->wall_u[0]), __ldg(&e->wall_u[1]), __ldg(&e->wall_u[2])};
       st_usqr = norm_sqr(wu);
       return true;
+    } else if (is_interpolated(kind)) {
+      if constexpr (KIND == K_BGK || KIND == K_TRT || KIND == K_SMAGORINSKY) {
+        collide_interpolated<L, KIND>(f, kind, e, x, y, z, st_rho, st_usqr);
+        return true;
+      }
     }
   }
   return false;  // NoDynamics / bounce-back: no statistic
@@ -487,6 +497,7 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
     };
     auto cell = [&](auto half_tag, int kind, const DynDevice<float>* pe) {
       constexpr bool HI = decltype(half_tag)::value;
+      const int x = HI ? xp + (g.nx >> 1) : xp;
       float f[Q];
       static_for<0, Q>([&](auto i) {
         constexpr int col = ODD ? L::opp(i) : i.value;
@@ -495,7 +506,7 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
         f[i] = (HI ? fv.y : fv.x) * inv;
       });
       float r = 0.f, u2 = 0.f;
-      const bool counted = collide_any<L, KIND, MASKED>(f, kind, pe, bulk, r, u2);
+      const bool counted = collide_any<L, KIND, MASKED>(f, kind, pe, bulk, x, y, z, r, u2);
       // repack: the written value is population i in column (ODD ? i : opp(i))
       static_for<0, Q>([&](auto i) {
         constexpr int col = ODD ? i.value : L::opp(i);
@@ -632,6 +643,10 @@ __global__ void moments_kernel(const S* __restrict__ pops, const Geometry g, boo
     rho = p->wall_rho; u[0] = u[1] = u[2] = R(0);
   } else if (kind == K_BOUNCE_BACK_VELOCITY) {
     rho = p->wall_rho; u[0] = p->wall_u[0]; u[1] = p->wall_u[1]; u[2] = p->wall_u[2];
+  } else if (is_interpolated(kind)) {
+    R f[Q];
+    static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted); });
+    bc_rho_u<L>(f, kind, p->bc_dir, p->bc_orient, p->bc_values + 4 * size_t(bc_index(p, x, y, z)), rho, u);
   } else {
     rho = R(1); u[0] = u[1] = u[2] = R(0);
   }
@@ -639,6 +654,190 @@ __global__ void moments_kernel(const S* __restrict__ pops, const Geometry g, boo
   u_out[n] = u[0];
   u_out[cells + n] = u[1];
   u_out[2 * cells + n] = u[2];
+}
+
+// ---------------------------------------------------------------------------
+// PostStream: PlaneFdBoundaryProcessor3D on the interpolated boundary cells
+//
+// src/boundary/boundaryPostProcessors3D.hh:39-92.  Each boundary cell is
+// rebuilt from the post-stream state as feq(rho, u) + fneq(Pi), Pi from the
+// finite-difference strain rate: one-sided second order along the normal
+// (cells x - orient e and x - 2 orient e), central across it
+// (fd::DirectedGradients3D, src/utilities/finiteDifference3D.h:58-200).
+// Two passes: the first stores the velocity of every boundary cell (its
+// momenta on the post-stream state), the second rebuilds every boundary cell;
+// a boundary cell never reads another boundary cell's populations in the
+// second pass, so the passes need no ordering among cells.
+
+// Logical population I of cell (x,y,z) written back (inverse of logical_pop).
+template <int Q, class S, class R, int I>
+OLB_DEV void logical_store(S* __restrict__ pops, const Geometry& g, int x, int y, int z, bool shifted, R v)
+{
+  using L = Lattice<Q>;
+  if (!shifted) {
+    Store<S, R>::template store<L, I>(pops + size_t(I) * g.stride + cell_slot(g, x, y, z), v);
+    return;
+  }
+  constexpr int o = L::opp(I);
+  const uint32_t dst = cell_slot(g, wrap(x - L::c(I, 0), g.nx), wrap(y - L::c(I, 1), g.ny),
+                                 wrap(z - L::c(I, 2), g.nz));
+  Store<S, R>::template store<L, o>(pops + size_t(o) * g.stride + dst, v);
+}
+
+// equilibrium<DESCRIPTOR>::fromPiToFneq  src/dynamics/lbm.h:225-247
+template <class L, int I, class R>
+OLB_DEV R from_pi_to_fneq(const R (&pi)[6])
+{
+  R fneq = R(0);
+  static_for<0, 3>([&](auto a) {
+    static_for<a.value, 3>([&](auto b) {
+      constexpr int k = a.value * 3 - (a.value * (a.value - 1)) / 2 + (b.value - a.value);
+      R to_add = R(L::c(I, a) * L::c(I, b));
+      if constexpr (a.value == b.value) {
+        to_add -= R(1) / R(3);
+      } else {
+        to_add *= R(2);
+      }
+      to_add *= pi[k];
+      fneq += to_add;
+    });
+  });
+  fneq *= weight<L, R>(I) * R(3) * R(3) / R(2);
+  return fneq;
+}
+
+OLB_DEV void decode_cell(const Geometry& g, uint32_t n, int& x, int& y, int& z)
+{
+  const uint32_t nynz = uint32_t(g.ny) * uint32_t(g.nz);
+  const uint32_t xx = n / nynz;
+  const uint32_t r = n - xx * nynz;
+  const uint32_t yy = r / uint32_t(g.nz);
+  x = int(xx);
+  y = int(yy);
+  z = int(r - yy * uint32_t(g.nz));
+}
+
+// Cell::computeU through the cell's dynamics on the post-stream state: bulk
+// (momenta/elements.h:466-475), forced bulk (:1480-1488), VELOCITY of moving
+// walls, the stored velocity of interpolated cells, zero otherwise.  A cell
+// beyond a non-periodic face is the reference's NoDynamics padding: zero.
+template <int Q, class S, class R>
+OLB_DEV void cell_velocity(const S* __restrict__ pops, const Geometry& g, bool shifted,
+                           const uint8_t* __restrict__ ids, const DynDevice<R>* __restrict__ table,
+                           int periodic, int x, int y, int z, R (&u)[3])
+{
+  using L = Lattice<Q>;
+  u[0] = u[1] = u[2] = R(0);
+  int p[3] = {x, y, z};
+  const int ext[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (p[d] < 0 || p[d] >= ext[d]) {
+      if (!((periodic >> d) & 1)) return;
+      p[d] = p[d] < 0 ? p[d] + ext[d] : p[d] - ext[d];
+    }
+  }
+  const uint32_t n = (uint32_t(p[0]) * uint32_t(g.ny) + uint32_t(p[1])) * uint32_t(g.nz) + uint32_t(p[2]);
+  const DynDevice<R>* e = table + ids[n];
+  const int kind = e->kind;
+  if (kind == K_BGK || kind == K_TRT || kind == K_SMAGORINSKY || kind == K_FORCED_BGK || kind == K_FORCED_TRT) {
+    R f[Q];
+    static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, p[0], p[1], p[2], shifted); });
+    R rho;
+    if (kind == K_FORCED_BGK || kind == K_FORCED_TRT) {
+      const R gg[3] = {e->force[0], e->force[1], e->force[2]};
+      compute_rho_u_forced<L>(f, gg, rho, u);
+    } else {
+      compute_rho_u<L>(f, rho, u);
+    }
+  } else if (kind == K_BOUNCE_BACK_VELOCITY) {
+    u[0] = e->wall_u[0]; u[1] = e->wall_u[1]; u[2] = e->wall_u[2];
+  } else if (is_interpolated(kind)) {
+    const R* bu = e->bc_u + 3 * size_t(bc_index(e, p[0], p[1], p[2]));
+    u[0] = bu[0]; u[1] = bu[1]; u[2] = bu[2];
+  }
+}
+
+// pass 1: velocity of every interpolated cell (its momenta, post-stream state)
+template <int Q, class S, class R>
+__global__ void bc_velocity_kernel(const S* __restrict__ pops, const Geometry g, bool shifted,
+                                   const uint8_t* __restrict__ ids, const DynDevice<R>* __restrict__ table,
+                                   const uint32_t* __restrict__ cells, uint32_t count)
+{
+  using L = Lattice<Q>;
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint32_t n = cells[k];
+  int x, y, z;
+  decode_cell(g, n, x, y, z);
+  const DynDevice<R>* e = table + ids[n];
+  const uint32_t bi = bc_index(e, x, y, z);
+  R f[Q];
+  static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted); });
+  R rho, u[3];
+  bc_rho_u<L>(f, e->kind, e->bc_dir, e->bc_orient, e->bc_values + 4 * size_t(bi), rho, u);
+  R* bu = e->bc_u + 3 * size_t(bi);
+  bu[0] = u[0];
+  bu[1] = u[1];
+  bu[2] = u[2];
+}
+
+// pass 2: PlaneFdBoundaryProcessor3D<direction,orientation>::apply
+template <int Q, class S, class R>
+__global__ void plane_fd_kernel(S* __restrict__ pops, const Geometry g, bool shifted,
+                                const uint8_t* __restrict__ ids, const DynDevice<R>* __restrict__ table,
+                                int periodic, const uint32_t* __restrict__ cells, uint32_t count)
+{
+  using L = Lattice<Q>;
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint32_t n = cells[k];
+  int x, y, z;
+  decode_cell(g, n, x, y, z);
+  const DynDevice<R>* e = table + ids[n];
+  const int dir = e->bc_dir, orient = e->bc_orient;
+  R f[Q];
+  static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted); });
+  R rho, u[3];
+  bc_rho_u<L>(f, e->kind, dir, orient, e->bc_values + 4 * size_t(bc_index(e, x, y, z)), rho, u);
+  // grad[d][c]: derivative along axis d of velocity component c
+  R grad[3][3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int ex = d == 0, ey = d == 1, ez = d == 2;
+    if (d == dir) {
+      const int s = -orient;
+      R u1[3], u2[3];
+      cell_velocity<Q, S, R>(pops, g, shifted, ids, table, periodic, x + s * ex, y + s * ey, z + s * ez, u1);
+      cell_velocity<Q, S, R>(pops, g, shifted, ids, table, periodic, x + 2 * s * ex, y + 2 * s * ey,
+                             z + 2 * s * ez, u2);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        grad[d][c] = R(-orient) * ((-R(3) * u[c] + R(4) * u1[c] - R(1) * u2[c]) / R(2));
+      }
+    } else {
+      R up[3], um[3];
+      cell_velocity<Q, S, R>(pops, g, shifted, ids, table, periodic, x + ex, y + ey, z + ez, up);
+      cell_velocity<Q, S, R>(pops, g, shifted, ids, table, periodic, x - ex, y - ey, z - ez, um);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        grad[d][c] = (up[c] - um[c]) / R(2);
+      }
+    }
+  }
+  const R s_to_pi = -rho / R(3) / e->omega;
+  R pi[6];
+  pi[0] = R(2) * grad[0][0] * s_to_pi;
+  pi[3] = R(2) * grad[1][1] * s_to_pi;
+  pi[5] = R(2) * grad[2][2] * s_to_pi;
+  pi[1] = (grad[0][1] + grad[1][0]) * s_to_pi;
+  pi[2] = (grad[0][2] + grad[2][0]) * s_to_pi;
+  pi[4] = (grad[1][2] + grad[2][1]) * s_to_pi;
+  const R usqr = norm_sqr(u);
+  static_for<0, Q>([&](auto i) {
+    const R v = feq2<L, i.value>(rho, u, usqr) + from_pi_to_fneq<L, i.value>(pi);
+    logical_store<Q, S, R, i.value>(pops, g, x, y, z, shifted, v);
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -670,6 +869,11 @@ cudaError_t launch_scatter(void* pops, const Geometry& g, const void* in, int i_
 template <int Q, class S, class R>
 cudaError_t launch_moments(const void* pops, const Geometry& g, bool shifted, const uint8_t* ids,
                            const void* table, void* rho, void* u, cudaStream_t stream);
+
+// both PostStream passes over `count` interpolated cells
+template <int Q, class S, class R>
+cudaError_t launch_boundary(void* pops, const Geometry& g, bool shifted, const uint8_t* ids, const void* table,
+                            int periodic, const uint32_t* cells, uint32_t count, cudaStream_t stream);
 
 inline dim3 step_grid(const Geometry& g, int bz, int by, int cells_per_thread)
 {

@@ -111,6 +111,23 @@ cudaError_t launch_moments(const void* pops, const Geometry& g, bool shifted, co
   return cudaGetLastError();
 }
 
+template <int Q, class S, class R>
+cudaError_t launch_boundary(void* pops, const Geometry& g, bool shifted, const uint8_t* ids, const void* table,
+                            int periodic, const uint32_t* cells, uint32_t count, cudaStream_t stream)
+{
+  if (count == 0) return cudaSuccess;
+  const int threads = 128;
+  const unsigned blocks = (count + threads - 1) / threads;
+  const auto* t = static_cast<const DynDevice<R>*>(table);
+  bc_velocity_kernel<Q, S, R><<<blocks, threads, 0, stream>>>(static_cast<const S*>(pops), g, shifted, ids, t,
+                                                              cells, count);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  plane_fd_kernel<Q, S, R><<<blocks, threads, 0, stream>>>(static_cast<S*>(pops), g, shifted, ids, t, periodic,
+                                                           cells, count);
+  return cudaGetLastError();
+}
+
 } // namespace olb_b200
 
 #define OLB_B200_INSTANTIATE(Q, S, R)                                                              \
@@ -122,4 +139,7 @@ cudaError_t launch_moments(const void* pops, const Geometry& g, bool shifted, co
                                                cudaStream_t);                                      \
   template cudaError_t launch_moments<Q, S, R>(const void*, const Geometry&, bool, const uint8_t*, \
                                                const void*, void*, void*, cudaStream_t);           \
+  template cudaError_t launch_boundary<Q, S, R>(void*, const Geometry&, bool, const uint8_t*,      \
+                                                const void*, int, const uint32_t*, uint32_t,       \
+                                                cudaStream_t);                                     \
   }

@@ -108,8 +108,11 @@ OLB_HD constexpr float storage_scale(int i)
 
 enum DynKind : int32_t {
   K_NONE = 0, K_BGK = 1, K_TRT = 2, K_SMAGORINSKY = 3, K_BOUNCE_BACK = 4,
-  K_BOUNCE_BACK_VELOCITY = 5, K_FORCED_BGK = 6, K_FORCED_TRT = 7
+  K_BOUNCE_BACK_VELOCITY = 5, K_FORCED_BGK = 6, K_FORCED_TRT = 7,
+  K_INTERP_VELOCITY = 8, K_INTERP_PRESSURE = 9
 };
+
+OLB_HD bool is_interpolated(int kind) { return kind == K_INTERP_VELOCITY || kind == K_INTERP_PRESSURE; }
 
 template <class R>
 struct DynDevice {
@@ -124,7 +127,21 @@ struct DynDevice {
   R wall_u[3];      // VELOCITY (moving wall)
   R wall_rho;       // RHO (FixedDensity)
   R wall_term[27][3]; // 2 rho u_d c_id w_i cs^-2, evaluated as the reference does (collision.h:341-343)
+  // interpolated velocity / pressure boundaries (flat faces)
+  int32_t bc_dir;     // axis of the outward normal
+  int32_t bc_orient;  // its sign, -1 or +1
+  int32_t box[6];     // x0, y0, z0 and extents of the bounding box of the entry's cells
+  const R* bc_values; // per box cell: RHO, VELOCITY x, y, z (4 values)
+  R* bc_u;            // per box cell: velocity of the post-stream state (3 values)
 };
+
+// index of cell (x,y,z) in the value box of its boundary entry
+template <class R>
+OLB_DEV uint32_t bc_index(const DynDevice<R>* e, int x, int y, int z)
+{
+  return (uint32_t(x - e->box[0]) * uint32_t(e->box[4]) + uint32_t(y - e->box[1])) * uint32_t(e->box[5]) +
+         uint32_t(z - e->box[2]);
+}
 
 // ---------------------------------------------------------------------------
 // moments
@@ -433,6 +450,86 @@ OLB_DEV void collide_bulk(R (&f)[L::q], const DynDevice<R>& p, R& st_rho, R& st_
     add_force<L>(f, rho, u, p.force_relax, g);
     st_rho = rho; st_usqr = norm_sqr(u);
   }
+}
+
+// ---------------------------------------------------------------------------
+// interpolated velocity / pressure boundaries on flat faces
+
+// Sums over the populations in the boundary plane (c_i[dir] == 0) and over
+// those along the outward normal (c_i[dir] == orient), each in ascending
+// population order: util::populationsContributingToVelocity
+// (src/core/util.h:221-229) as velocityBMRho and FixedPressureMomentum use
+// them (src/dynamics/momenta/elements.h:54-71, 604-621).
+template <class L, class R>
+OLB_DEV void bc_sums(const R (&f)[L::q], int dir, int orient, R& on_wall, R& normal)
+{
+  on_wall = R(0);
+  normal = R(0);
+  static_for<0, L::q>([&](auto i) {
+    constexpr int c0 = L::c(i, 0), c1 = L::c(i, 1), c2 = L::c(i, 2);
+    const int cd = dir == 0 ? c0 : (dir == 1 ? c1 : c2);
+    if (cd == 0) {
+      on_wall += f[i];
+    } else if (cd == orient) {
+      normal += f[i];
+    }
+  });
+}
+
+// computeRhoU of the exchanged momenta (generic ComputeRhoU,
+// src/dynamics/momenta/interface.h:50-58); v = {RHO, VELOCITY x, y, z}:
+//   velocity  BasicDirichletVelocityBoundaryTuple (momenta/aliases.h:146-151):
+//             u = VELOCITY, rho = velocityBMRho(cell, u) (elements.h:54-71, 325-333)
+//   pressure  BasicDirichletPressureBoundaryTuple (momenta/aliases.h:166-171):
+//             rho = RHO, u = VELOCITY but u[dir] from the populations
+//             (FixedPressureMomentum::computeU, elements.h:596-622)
+template <class L, class R>
+OLB_DEV void bc_rho_u(const R (&f)[L::q], int kind, int dir, int orient, const R* __restrict__ v, R& rho,
+                      R (&u)[3])
+{
+  R on_wall, normal;
+  bc_sums<L>(f, dir, orient, on_wall, normal);
+  u[0] = v[1];
+  u[1] = v[2];
+  u[2] = v[3];
+  const R so = R(orient);
+  if (kind == K_INTERP_VELOCITY) {
+    const R ud = dir == 0 ? u[0] : (dir == 1 ? u[1] : u[2]);
+    rho = (R(2) * normal + on_wall + R(1)) / (R(1) + so * ud);
+  } else {
+    rho = v[0];
+    const R un = so * ((R(2) * normal + on_wall + R(1)) / rho - R(1));
+    if (dir == 0) {
+      u[0] = un;
+    } else if (dir == 1) {
+      u[1] = un;
+    } else {
+      u[2] = un;
+    }
+  }
+}
+
+// MixinDynamics::exchange_momenta<...>: the mixin collision (the lattice's
+// fluid collision KIND) evaluated with the boundary momenta — BGK
+// (collision.h:67-78), TRT (:220-245) or Smagorinsky-BGK (collisionLES.h:59-89,
+// whose stress is BulkStress of the same rho and u).
+template <class L, int KIND, class R>
+OLB_DEV void collide_interpolated(R (&f)[L::q], int kind, const DynDevice<R>* __restrict__ e, int x, int y,
+                                  int z, R& st_rho, R& st_usqr)
+{
+  const R* __restrict__ v = e->bc_values + 4 * size_t(bc_index(e, x, y, z));
+  R rho, u[3];
+  bc_rho_u<L>(f, kind, e->bc_dir, e->bc_orient, v, rho, u);
+  if constexpr (KIND == K_TRT) {
+    relax_trt<L>(f, rho, u, e->omega, e->omega_minus);
+  } else if constexpr (KIND == K_SMAGORINSKY) {
+    const R w = smagorinsky_omega<L>(f, rho, u, e->smago_pre, e->tau_mol);
+    relax_bgk<L>(f, rho, u, w);
+  } else {
+    relax_bgk<L>(f, rho, u, e->omega);
+  }
+  st_rho = rho;
+  st_usqr = norm_sqr(u);
 }
 
 // collision::NguyenLaddCorrection<Revert>  src/dynamics/collision.h:333-346

@@ -29,7 +29,10 @@ namespace olb_b200 {
                                                       int, cudaStream_t);                          \
   extern template cudaError_t launch_moments<Q, S, R>(const void*, const Geometry&, bool,          \
                                                       const uint8_t*, const void*, void*, void*,   \
-                                                      cudaStream_t);
+                                                      cudaStream_t);                               \
+  extern template cudaError_t launch_boundary<Q, S, R>(void*, const Geometry&, bool, const uint8_t*, \
+                                                       const void*, int, const uint32_t*, uint32_t, \
+                                                       cudaStream_t);
 OLB_B200_EXTERN(19, float, float)
 OLB_B200_EXTERN(19, double, double)
 OLB_B200_EXTERN(19, __half, float)
@@ -222,6 +225,21 @@ struct olb_b200_lattice {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   size_t device_bytes = 0;
+  // interpolated velocity / pressure boundaries
+  struct BcBox {
+    int box[6];             // x0, y0, z0, extents (0 extents: not a boundary entry)
+    size_t slot0;           // first value slot
+  };
+  std::vector<BcBox> bc_box;        // per table entry
+  std::vector<uint8_t> ids_host;    // per cell (kept while boundary entries exist)
+  std::vector<double> bc_host;      // 4 values per slot, host copy
+  uint32_t* bc_cells = nullptr;     // device: cell index of every boundary cell
+  uint32_t n_bc = 0;
+  void* bc_values = nullptr;        // device: 4 R per slot
+  void* bc_u = nullptr;             // device: 3 R per slot
+  size_t bc_slots = 0;
+  size_t bc_bytes = 0;
+  bool initialized = false;         // PostStream post-processors applied to the initial state
 };
 
 namespace {
@@ -294,6 +312,37 @@ olb_b200_status ensure_partial_count(olb_b200_lattice* L, size_t need)
   return OLB_B200_OK;
 }
 
+olb_b200_status upload_boundary_values(olb_b200_lattice* L);
+
+int periodic_mask(const olb_b200_lattice* L)
+{
+  return (L->desc.periodic[0] ? 1 : 0) | (L->desc.periodic[1] ? 2 : 0) | (L->desc.periodic[2] ? 4 : 0);
+}
+
+// The PostStream stage (SuperLattice::collideAndStream, src/core/superLattice.hh:640-641):
+// PlaneFdBoundaryProcessor3D on every interpolated boundary cell.
+olb_b200_status post_stream(olb_b200_lattice* L)
+{
+  if (L->n_bc == 0) return OLB_B200_OK;
+  cudaError_t e = dispatch(L, [&](auto qc, auto s_, auto r_) {
+    return launch_boundary<decltype(qc)::value, decltype(s_), decltype(r_)>(
+      L->pops, L->g, L->parity == 1, L->ids, L->table, periodic_mask(L), L->bc_cells, L->n_bc, L->stream);
+  });
+  if (e != cudaSuccess) return cuda_fail(e, "boundary post-processing kernels");
+  return OLB_B200_OK;
+}
+
+// BlockLattice::initialize (src/core/blockLattice.hh:56-67): the PostStream
+// post-processors run once on the initial state, before the first collision.
+olb_b200_status initialize_once(olb_b200_lattice* L)
+{
+  if (L->initialized) return OLB_B200_OK;
+  olb_b200_status st = post_stream(L);
+  if (st != OLB_B200_OK) return st;
+  L->initialized = true;
+  return OLB_B200_OK;
+}
+
 olb_b200_status enqueue_steps(olb_b200_lattice* L, int steps, bool stats_last)
 {
   for (int s = 0; s < steps; ++s) {
@@ -318,8 +367,102 @@ olb_b200_status enqueue_steps(olb_b200_lattice* L, int steps, bool stats_last)
     if (e != cudaSuccess) return cuda_fail(e, "step kernel launch");
     L->parity ^= 1;
     L->steps_done += 1;
+    olb_b200_status st = post_stream(L);
+    if (st != OLB_B200_OK) return st;
   }
   return OLB_B200_OK;
+}
+
+// Per boundary entry: the bounding box of its cells, which indexes its values
+// (RHO, VELOCITY per cell, as defineRho / defineU set them); the list of all
+// boundary cells for the PostStream passes.  Values start at RHO = 1, VELOCITY
+// = 0 (FixedDensity / FixedVelocityMomentumGeneric::initialize,
+// src/dynamics/momenta/elements.h:251-255, 560-565).
+olb_b200_status setup_boundaries(olb_b200_lattice* L, const uint8_t* ids, const olb_b200_dyn_params* table,
+                                 int n_entries, bool any)
+{
+  if (L->bc_cells) cudaFree(L->bc_cells);
+  if (L->bc_values) cudaFree(L->bc_values);
+  if (L->bc_u) cudaFree(L->bc_u);
+  L->bc_cells = nullptr;
+  L->bc_values = nullptr;
+  L->bc_u = nullptr;
+  L->device_bytes -= L->bc_bytes;
+  L->bc_bytes = 0;
+  L->n_bc = 0;
+  L->bc_slots = 0;
+  L->bc_box.assign(size_t(n_entries), olb_b200_lattice::BcBox{{0, 0, 0, 0, 0, 0}, 0});
+  L->bc_host.clear();
+  L->ids_host.clear();
+  if (!any) return OLB_B200_OK;
+  const int nx = L->desc.nx, ny = L->desc.ny, nz = L->desc.nz;
+  std::vector<int> lo(size_t(n_entries) * 3, INT32_MAX), hi(size_t(n_entries) * 3, -1);
+  std::vector<uint32_t> cells;
+  for (int x = 0; x < nx; ++x) {
+    for (int y = 0; y < ny; ++y) {
+      for (int z = 0; z < nz; ++z) {
+        const size_t c = (size_t(x) * ny + y) * nz + z;
+        const int k = ids[c];
+        if (!is_interpolated(table[k].kind)) continue;
+        cells.push_back(uint32_t(c));
+        const int p[3] = {x, y, z};
+        for (int d = 0; d < 3; ++d) {
+          lo[3 * k + d] = std::min(lo[3 * k + d], p[d]);
+          hi[3 * k + d] = std::max(hi[3 * k + d], p[d]);
+        }
+      }
+    }
+  }
+  size_t slots = 0;
+  for (int k = 0; k < n_entries; ++k) {
+    if (hi[3 * k] < 0) continue;
+    auto& b = L->bc_box[size_t(k)];
+    for (int d = 0; d < 3; ++d) {
+      b.box[d] = lo[3 * k + d];
+      b.box[3 + d] = hi[3 * k + d] - lo[3 * k + d] + 1;
+    }
+    b.slot0 = slots;
+    slots += size_t(b.box[3]) * b.box[4] * b.box[5];
+  }
+  if (cells.empty()) return OLB_B200_OK;
+  L->ids_host.assign(ids, ids + L->cells);
+  L->bc_slots = slots;
+  L->bc_host.assign(4 * slots, 0.0);
+  for (size_t k = 0; k < slots; ++k) L->bc_host[4 * k] = 1.0;
+  L->n_bc = uint32_t(cells.size());
+  OLB_CUDA(cudaMalloc(&L->bc_cells, cells.size() * sizeof(uint32_t)));
+  OLB_CUDA(cudaMalloc(&L->bc_values, 4 * slots * L->real));
+  OLB_CUDA(cudaMalloc(&L->bc_u, 3 * slots * L->real));
+  OLB_CUDA(cudaMemset(L->bc_u, 0, 3 * slots * L->real));
+  L->bc_bytes = cells.size() * sizeof(uint32_t) + 7 * slots * L->real;
+  L->device_bytes += L->bc_bytes;
+  OLB_CUDA(cudaMemcpy(L->bc_cells, cells.data(), cells.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  return upload_boundary_values(L);
+}
+
+olb_b200_status upload_boundary_values(olb_b200_lattice* L)
+{
+  if (!L->bc_slots) return OLB_B200_OK;
+  if (L->real == 8) {
+    OLB_CUDA(cudaMemcpy(L->bc_values, L->bc_host.data(), L->bc_host.size() * sizeof(double),
+                        cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> v(L->bc_host.begin(), L->bc_host.end());
+    OLB_CUDA(cudaMemcpy(L->bc_values, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  return OLB_B200_OK;
+}
+
+template <class R>
+void attach_boundary(const olb_b200_lattice* L, int k, const olb_b200_dyn_params& in, DynDevice<R>& d)
+{
+  if (!is_interpolated(in.kind)) return;
+  const auto& b = L->bc_box[size_t(k)];
+  d.bc_dir = in.direction;
+  d.bc_orient = in.orientation;
+  for (int e = 0; e < 6; ++e) d.box[e] = b.box[e];
+  d.bc_values = L->bc_values ? static_cast<const R*>(L->bc_values) + 4 * b.slot0 : nullptr;
+  d.bc_u = L->bc_u ? static_cast<R*>(L->bc_u) + 3 * b.slot0 : nullptr;
 }
 
 } // namespace
@@ -422,6 +565,9 @@ void olb_b200_destroy(olb_b200_lattice* L)
   if (L->scratch) cudaFree(L->scratch);
   if (L->partials) cudaFree(L->partials);
   if (L->uprev) cudaFree(L->uprev);
+  if (L->bc_cells) cudaFree(L->bc_cells);
+  if (L->bc_values) cudaFree(L->bc_values);
+  if (L->bc_u) cudaFree(L->bc_u);
   if (L->stat_dev) cudaFree(L->stat_dev);
   if (L->stat_host) cudaFreeHost(L->stat_host);
   if (L->ev0) cudaEventDestroy(L->ev0);
@@ -437,11 +583,29 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
   if (!L || !table) return fail(OLB_B200_ERR_ARG, "set_dynamics: null argument");
   if (n_entries < 1 || n_entries > 256)
     return fail(OLB_B200_ERR_ARG, "set_dynamics: table needs 1..256 entries, got %d", n_entries);
-  int bulk = -1;
+  int bulk = -1, first_bc = -1;
   for (int k = 0; k < n_entries; ++k) {
     const int kind = table[k].kind;
-    if (kind < OLB_B200_DYN_NONE || kind > OLB_B200_DYN_FORCED_TRT)
+    if (kind < OLB_B200_DYN_NONE || kind > OLB_B200_DYN_INTERPOLATED_PRESSURE)
       return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d has unknown kind %d", k, kind);
+    if (is_interpolated(kind)) {
+      const int m = table[k].mixin;
+      if (m != OLB_B200_DYN_BGK && m != OLB_B200_DYN_TRT && m != OLB_B200_DYN_SMAGORINSKY)
+        return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: entry %d: interpolated boundaries take a BGK, TRT "
+                    "or Smagorinsky-BGK mixin, got kind %d", k, m);
+      if (table[k].direction < 0 || table[k].direction > 2 ||
+          (table[k].orientation != 1 && table[k].orientation != -1))
+        return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d: normal axis %d / sign %d invalid", k,
+                    table[k].direction, table[k].orientation);
+      if (!(table[k].omega > 0.0 && table[k].omega < 2.0))
+        return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d omega %g outside (0,2)", k, table[k].omega);
+      if (first_bc < 0) {
+        first_bc = k;
+      } else if (table[first_bc].mixin != m) {
+        return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: entries %d and %d use different boundary mixins",
+                    first_bc, k);
+      }
+    }
     if (is_fluid(kind)) {
       if (!(table[k].omega > 0.0 && table[k].omega < 2.0))
         return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d omega %g outside (0,2)", k, table[k].omega);
@@ -453,6 +617,12 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
                     "fluid collision kind per lattice is supported", bulk, k, table[bulk].kind, kind);
       }
     }
+  }
+  if (first_bc >= 0) {
+    if (bulk >= 0 && table[bulk].kind != table[first_bc].mixin)
+      return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: the boundary mixin (kind %d) must be the lattice's "
+                  "fluid collision (kind %d)", table[first_bc].mixin, table[bulk].kind);
+    if (!ids) return fail(OLB_B200_ERR_ARG, "set_dynamics: interpolated boundaries need per-cell ids");
   }
   bool uniform = ids == nullptr;
   uint8_t first = 0;
@@ -467,15 +637,20 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
   }
   olb_b200_status st = select_device(L);
   if (st != OLB_B200_OK) return st;
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  st = setup_boundaries(L, ids, table, n_entries, first_bc >= 0);
+  if (st != OLB_B200_OK) return st;
   // device table and the host copy of the bulk entry
   const bool f64 = L->desc.storage == OLB_B200_STORAGE_F64;
   std::vector<unsigned char> host(size_t(n_entries) * (f64 ? sizeof(DynDevice<double>) : sizeof(DynDevice<float>)));
   for (int k = 0; k < n_entries; ++k) {
     if (f64) {
       auto d = make_device_params<double>(L->q, table[k]);
+      attach_boundary(L, k, table[k], d);
       std::memcpy(host.data() + k * sizeof d, &d, sizeof d);
     } else {
       auto d = make_device_params<float>(L->q, table[k]);
+      attach_boundary(L, k, table[k], d);
       std::memcpy(host.data() + k * sizeof d, &d, sizeof d);
     }
   }
@@ -486,8 +661,8 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
   } else {
     OLB_CUDA(cudaMemset(L->ids, 0, L->cells));
   }
-  const int bulk_entry = bulk >= 0 ? bulk : 0;
-  L->bulk_kind = bulk >= 0 ? table[bulk].kind : K_BGK;
+  const int bulk_entry = bulk >= 0 ? bulk : (first_bc >= 0 ? first_bc : 0);
+  L->bulk_kind = bulk >= 0 ? table[bulk].kind : (first_bc >= 0 ? table[first_bc].mixin : K_BGK);
   const size_t esz = f64 ? sizeof(DynDevice<double>) : sizeof(DynDevice<float>);
   std::memcpy(L->bulk, host.data() + bulk_entry * esz, esz);
   // the unmasked kernel serves lattices where every cell uses one fluid entry
@@ -581,6 +756,8 @@ olb_b200_status olb_b200_collide_and_stream(olb_b200_lattice* L, int32_t steps, 
     st = ensure_partials(L);
     if (st != OLB_B200_OK) return st;
   }
+  st = initialize_once(L);
+  if (st != OLB_B200_OK) return st;
   st = enqueue_steps(L, steps, stats != nullptr);
   if (st != OLB_B200_OK) return st;
   if (!stats) return OLB_B200_OK;
@@ -641,6 +818,8 @@ olb_b200_status olb_b200_time_steps(olb_b200_lattice* L, int32_t steps, float* m
   g_last_error.clear();
   if (!L || !ms || steps < 1) return fail(OLB_B200_ERR_ARG, "time_steps: bad argument");
   olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  st = initialize_once(L);
   if (st != OLB_B200_OK) return st;
   OLB_CUDA(cudaStreamSynchronize(L->stream));
   OLB_CUDA(cudaEventRecord(L->ev0, L->stream));
@@ -725,6 +904,46 @@ olb_b200_status olb_b200_velocity_residual(olb_b200_lattice* L, double* residual
   OLB_CUDA(cudaStreamSynchronize(L->stream));
   const StatPartial p = *L->stat_host;
   *residual = p.sum_usqr > 0. ? std::sqrt(p.sum_rho / p.sum_usqr) : (p.sum_rho > 0. ? INFINITY : 0.);
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_set_boundary_values(olb_b200_lattice* L, const int64_t* cells, int64_t count,
+                                             const double* values)
+{
+  g_last_error.clear();
+  if (!L || (count > 0 && (!cells || !values))) return fail(OLB_B200_ERR_ARG, "set_boundary_values: null argument");
+  if (count < 0) return fail(OLB_B200_ERR_ARG, "set_boundary_values: negative count");
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  const int ny = L->desc.ny, nz = L->desc.nz;
+  for (int64_t j = 0; j < count; ++j) {
+    const int64_t c = cells[j];
+    if (c < 0 || size_t(c) >= L->cells)
+      return fail(OLB_B200_ERR_ARG, "set_boundary_values: cell %lld out of range", (long long)c);
+    if (L->ids_host.empty() || L->bc_box[L->ids_host[size_t(c)]].box[3] == 0)
+      return fail(OLB_B200_ERR_ARG, "set_boundary_values: cell %lld is not an interpolated boundary cell",
+                  (long long)c);
+    const auto& b = L->bc_box[L->ids_host[size_t(c)]];
+    const int x = int(c / (int64_t(ny) * nz));
+    const int y = int((c / nz) % ny);
+    const int z = int(c % nz);
+    const size_t slot = b.slot0 + (size_t(x - b.box[0]) * b.box[4] + size_t(y - b.box[1])) * b.box[5] +
+                        size_t(z - b.box[2]);
+    for (int e = 0; e < 4; ++e) L->bc_host[4 * slot + e] = values[4 * j + e];
+  }
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  return upload_boundary_values(L);
+}
+
+olb_b200_status olb_b200_initialize(olb_b200_lattice* L)
+{
+  g_last_error.clear();
+  if (!L) return fail(OLB_B200_ERR_ARG, "initialize: null lattice");
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  st = initialize_once(L);
+  if (st != OLB_B200_OK) return st;
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
   return OLB_B200_OK;
 }
 

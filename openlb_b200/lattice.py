@@ -38,10 +38,16 @@ class Dynamics:
     force: tuple = (0.0, 0.0, 0.0)
     wall_u: tuple = (0.0, 0.0, 0.0)
     wall_rho: float = 1.0
+    mixin: int = 0          # interpolated boundaries: the mixin's collision kind
+    direction: int = 0      # interpolated boundaries: outward normal axis
+    orientation: int = 0    # interpolated boundaries: outward normal sign
 
     def params(self, omega_default: float | None = None) -> _abi.DynParams:
         p = _abi.DynParams()
         p.kind = self.kind
+        p.mixin = int(self.mixin)
+        p.direction = int(self.direction)
+        p.orientation = int(self.orientation)
         omega = self.omega if self.omega is not None else omega_default
         p.omega = float(omega) if omega is not None else 1.0
         p.magic = float(self.magic)
@@ -83,6 +89,21 @@ def BounceBack(rho: float = 1.0) -> Dynamics:
 
 def BounceBackVelocity(u=(0.0, 0.0, 0.0), rho: float = 1.0) -> Dynamics:
     return Dynamics(_abi.DYN_BOUNCE_BACK_VELOCITY, wall_u=tuple(u), wall_rho=rho)
+
+
+def InterpolatedVelocityBoundary(mixin: Dynamics, direction: int, orientation: int) -> Dynamics:
+    """A flat interpolated-velocity boundary entry: ``mixin`` collision with
+    BasicDirichletVelocityBoundaryTuple<direction,orientation> momenta and
+    PlaneFdBoundaryProcessor3D (src/boundary/interpolatedVelocity3D.h:44-81)."""
+    return Dynamics(_abi.DYN_INTERPOLATED_VELOCITY, omega=mixin.omega, magic=mixin.magic,
+                    smagorinsky=mixin.smagorinsky, mixin=mixin.kind, direction=direction, orientation=orientation)
+
+
+def InterpolatedPressureBoundary(mixin: Dynamics, direction: int, orientation: int) -> Dynamics:
+    """A flat interpolated-pressure boundary entry (BasicDirichletPressureBoundaryTuple,
+    src/boundary/interpolatedPressure3D.h:47-90)."""
+    return Dynamics(_abi.DYN_INTERPOLATED_PRESSURE, omega=mixin.omega, magic=mixin.magic,
+                    smagorinsky=mixin.smagorinsky, mixin=mixin.kind, direction=direction, orientation=orientation)
 
 
 FLUID_KINDS = {_abi.DYN_BGK, _abi.DYN_TRT, _abi.DYN_SMAGORINSKY, _abi.DYN_FORCED_BGK, _abi.DYN_FORCED_TRT}
@@ -152,6 +173,21 @@ class Lattice:
                 raise ValueError(f"ids has {ids.size} entries, lattice has {self.n} cells")
             ptr = ids.ctypes.data
         self._check(self._lib.olb_b200_set_dynamics(self._h, ptr, params, len(table)))
+
+    def set_boundary_values(self, cells: np.ndarray, values: np.ndarray) -> None:
+        """RHO and VELOCITY of interpolated boundary cells: values[j] =
+        (rho, ux, uy, uz) of logical cell index cells[j]."""
+        cells = np.ascontiguousarray(cells, dtype=np.int64).reshape(-1)
+        values = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        if values.size != 4 * cells.size:
+            raise ValueError(f"{cells.size} cells need {4 * cells.size} values, got {values.size}")
+        self._check(self._lib.olb_b200_set_boundary_values(self._h, cells.ctypes.data, cells.size,
+                                                           values.ctypes.data))
+
+    def initialize(self) -> None:
+        """SuperLattice::initialize: the PostStream post-processors once on the
+        current state (done by the first collide_and_stream otherwise)."""
+        self._check(self._lib.olb_b200_initialize(self._h))
 
     def set_launch_shape(self, block_z: int, block_y: int) -> None:
         self._check(self._lib.olb_b200_set_launch_shape(self._h, block_z, block_y))
@@ -327,6 +363,28 @@ class SuperLattice:
         self._pending_pops = np.zeros((self.descriptor.q, self.block.n), self.block.dtype)
         self._initialized = False
         self._statistics = None
+        self._bc: dict[int, tuple] = {}          # material -> (kind, mixin Dynamics or None)
+        self._bc_values = None                    # (4, n): RHO, VELOCITY of boundary cells
+
+    # boundary::set<InterpolatedVelocity / InterpolatedPressure>(sLattice, superGeometry, material)
+    def setBoundary(self, geometry: SuperGeometry, material: int, kind: int, mixin: Dynamics | None = None) -> None:
+        if kind not in _abi.DYN_INTERPOLATED:
+            raise ValueError(f"unknown boundary kind {kind}")
+        self._bc[int(material)] = (kind, mixin)
+
+    def _values(self):
+        if self._bc_values is None:
+            self._bc_values = np.zeros((4, self.block.n))
+            self._bc_values[0] = 1.0
+        return self._bc_values
+
+    def _bc_cells(self, material: int) -> np.ndarray:
+        return np.flatnonzero(self.geometry.materials.reshape(-1) == int(material))
+
+    def _push_values(self, material: int) -> None:
+        if self._initialized and int(material) in self._bc:
+            cells = self._bc_cells(material)
+            self.block.set_boundary_values(cells, self._values()[:, cells].T)
 
     # defineDynamics<DYNAMICS>(superGeometry, material)  superLattice.hh:286-291
     def defineDynamics(self, geometry: SuperGeometry, material: int, dynamics: Dynamics) -> None:
@@ -340,12 +398,29 @@ class SuperLattice:
     def defineForce(self, geometry: SuperGeometry, material: int, force) -> None:
         self._force[int(material)] = tuple(float(f) for f in force)
 
-    # defineU(superGeometry, material, u) on BounceBackVelocity cells
+    # defineU(superGeometry, material, u): the VELOCITY field of moving walls,
+    # or per cell on interpolated boundaries (u: a 3-vector or a (3, nx, ny, nz) field)
     def defineU(self, geometry: SuperGeometry, material: int, u) -> None:
-        self._wall_u[int(material)] = tuple(float(v) for v in u)
+        m = int(material)
+        if m in self._bc:
+            cells = self._bc_cells(m)
+            ua = np.asarray(u, dtype=np.float64)
+            ua = ua.reshape(3, 1) if ua.size == 3 else ua.reshape(3, -1)[:, cells]
+            self._values()[1:, cells] = ua
+            self._push_values(m)
+            return
+        self._wall_u[m] = tuple(float(v) for v in u)
 
-    def defineRho(self, geometry: SuperGeometry, material: int, rho: float) -> None:
-        self._wall_rho[int(material)] = float(rho)
+    # defineRho(superGeometry, material, rho): FixedDensity RHO (walls, pressure boundaries)
+    def defineRho(self, geometry: SuperGeometry, material: int, rho) -> None:
+        m = int(material)
+        if m in self._bc:
+            cells = self._bc_cells(m)
+            ra = np.asarray(rho, dtype=np.float64)
+            self._values()[0, cells] = ra if ra.size == 1 else ra.reshape(-1)[cells]
+            self._push_values(m)
+            return
+        self._wall_rho[m] = float(rho)
 
     # iniEquilibrium(superGeometry, material, rhoF, uF)  superLattice.hh:542-577
     def iniEquilibrium(self, geometry: SuperGeometry, material: int, rho, u) -> None:
@@ -362,15 +437,40 @@ class SuperLattice:
             self.block.set_populations(self._pending_pops.reshape(-1))
 
     def _table(self):
-        return dynamics_table(self.geometry.materials, self._dyn_of_material, self._params,
-                              self._force, self._wall_u, self._wall_rho)
+        table, ids = dynamics_table(self.geometry.materials, self._dyn_of_material, self._params,
+                                    self._force, self._wall_u, self._wall_rho)
+        # interpolated boundaries: one entry per material and discrete normal
+        from . import boundary
+        for m, (kind, mixin) in sorted(self._bc.items()):
+            mix = mixin if mixin is not None else BGKdynamics()
+            kw = {}
+            if mix.omega is None:
+                kw["omega"] = self._params.get("OMEGA")
+            if "MAGIC" in self._params:
+                kw["magic"] = self._params["MAGIC"]
+            if "SMAGORINSKY" in self._params:
+                kw["smagorinsky"] = self._params["SMAGORINSKY"]
+            if kw:
+                mix = Dynamics(**{**mix.__dict__, **kw})
+            make = InterpolatedVelocityBoundary if kind == _abi.DYN_INTERPOLATED_VELOCITY else \
+                InterpolatedPressureBoundary
+            for (axis, sign), cells in boundary.normal_groups(self.geometry.materials, self.geometry.periodic,
+                                                              m).items():
+                if len(table) >= 256:
+                    raise ValueError("more than 256 dynamics entries")
+                ids[cells] = len(table)
+                table.append(make(mix, axis, sign))
+        return table, ids
 
-    # initialize()  superLattice.hh:190-204
+    # initialize()  superLattice.hh:190-204, blockLattice.hh:56-67
     def initialize(self) -> None:
         table, ids = self._table()
         self.block.set_dynamics(table, ids)
-        self.block.set_populations(self._pending_pops.reshape(-1))
         self._initialized = True
+        for m in self._bc:
+            self._push_values(m)
+        self.block.set_populations(self._pending_pops.reshape(-1))
+        self.block.initialize()
 
     # collideAndStream()  superLattice.hh:601-663
     def collideAndStream(self, steps: int = 1, statistics: bool = False):
@@ -405,6 +505,7 @@ class SuperLattice:
 
 __all__ = [
     "Dynamics", "NoDynamics", "BGKdynamics", "TRTdynamics", "ForcedTRTdynamics", "ForcedBGKdynamics",
-    "SmagorinskyBGKdynamics", "BounceBack", "BounceBackVelocity", "Lattice", "SuperGeometry",
+    "SmagorinskyBGKdynamics", "BounceBack", "BounceBackVelocity", "InterpolatedVelocityBoundary",
+    "InterpolatedPressureBoundary", "Lattice", "SuperGeometry",
     "SuperLattice", "D3Q19", "D3Q27",
 ]

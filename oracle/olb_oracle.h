@@ -34,18 +34,24 @@ enum {
   ORACLE_BOUNCE_BACK = 4,          /* BounceBack                dynamics/dynamics.h:472-483 */
   ORACLE_BOUNCE_BACK_VELOCITY = 5, /* BounceBackVelocity        dynamics/dynamics.h:549-555 */
   ORACLE_FORCED_BGK = 6,           /* ForcedBGKdynamics         dynamics/dynamics.h:214 */
-  ORACLE_FORCED_TRT = 7            /* ForcedTRTdynamics         dynamics/dynamics.h:457-464 */
+  ORACLE_FORCED_TRT = 7,           /* ForcedTRTdynamics         dynamics/dynamics.h:457-464 */
+  /* flat-face interpolated boundaries: the mixin collision with exchanged
+   * momenta, plus PlaneFdBoundaryProcessor3D after every stream */
+  ORACLE_INTERP_VELOCITY = 8,      /* boundary::InterpolatedVelocity  boundary/interpolatedVelocity3D.h:44-50,78-81 */
+  ORACLE_INTERP_PRESSURE = 9       /* boundary::InterpolatedPressure  boundary/interpolatedPressure3D.h:47-90 */
 };
 
 typedef struct {
   int32_t kind;
-  int32_t pad_;
+  int32_t mixin;       /* interpolated boundaries: collision of the mixin dynamics (BGK, TRT, SMAGORINSKY) */
   double omega;        /* OMEGA */
   double magic;        /* collision::TRT::MAGIC */
   double smagorinsky;  /* collision::LES::SMAGORINSKY */
   double force[3];     /* FORCE field value (Guo forcing) */
   double wall_u[3];    /* VELOCITY field of moving-wall bounce-back */
   double wall_rho;     /* FixedDensity RHO field (1 after initialize) */
+  int32_t direction;   /* interpolated boundaries: axis of the outward normal */
+  int32_t orientation; /* interpolated boundaries: its sign, -1 or +1 */
 } oracle_dyn;
 
 typedef struct {
@@ -55,6 +61,9 @@ typedef struct {
   int32_t n_dyn;
   const uint8_t* dyn_id; /* per cell index into table, or NULL = all 0 */
   const oracle_dyn* table;
+  /* boundary values of interpolated cells, [4][cells]: RHO (fixed density of
+   * pressure cells), then the VELOCITY field x, y, z; NULL if none */
+  const double* bc_values;
 } oracle_lattice;
 
 typedef struct {
@@ -72,6 +81,12 @@ int oracle_step_f32(const oracle_lattice* lat, float* pops, int steps, float gho
                     oracle_stats* stats);
 int oracle_step_f64(const oracle_lattice* lat, double* pops, int steps, double ghost,
                     oracle_stats* stats);
+
+/* The PostStream post-processors alone (PlaneFdBoundaryProcessor3D on every
+ * interpolated cell), as BlockLattice::initialize() runs them once on the
+ * initial state (core/blockLattice.hh:56-67) before the first collision. */
+int oracle_post_process_f32(const oracle_lattice* lat, float* pops);
+int oracle_post_process_f64(const oracle_lattice* lat, double* pops);
 
 /* Density / velocity as OpenLB's Density3D/Velocity3D functors report them
  * (per-dynamics momenta: bulk, forced, fixed density, wall velocity, none). */

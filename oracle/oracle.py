@@ -24,20 +24,24 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "_build" / "libolb_oracle.so"
 REF_DIR = HERE / "_ref"
 
-NONE, BGK, TRT, SMAGORINSKY, BOUNCE_BACK, BOUNCE_BACK_VELOCITY, FORCED_BGK, FORCED_TRT = range(8)
+(NONE, BGK, TRT, SMAGORINSKY, BOUNCE_BACK, BOUNCE_BACK_VELOCITY, FORCED_BGK, FORCED_TRT,
+ INTERP_VELOCITY, INTERP_PRESSURE) = range(10)
 KIND_NAMES = {
     NONE: "none", BGK: "bgk", TRT: "trt", SMAGORINSKY: "smagorinsky",
     BOUNCE_BACK: "bounce_back", BOUNCE_BACK_VELOCITY: "bounce_back_velocity",
     FORCED_BGK: "forced_bgk", FORCED_TRT: "forced_trt",
+    INTERP_VELOCITY: "interpolated_velocity", INTERP_PRESSURE: "interpolated_pressure",
 }
+INTERPOLATED = (INTERP_VELOCITY, INTERP_PRESSURE)
 
 
 class _Dyn(ctypes.Structure):
     _fields_ = [
-        ("kind", ctypes.c_int32), ("pad_", ctypes.c_int32),
+        ("kind", ctypes.c_int32), ("mixin", ctypes.c_int32),
         ("omega", ctypes.c_double), ("magic", ctypes.c_double),
         ("smagorinsky", ctypes.c_double), ("force", ctypes.c_double * 3),
         ("wall_u", ctypes.c_double * 3), ("wall_rho", ctypes.c_double),
+        ("direction", ctypes.c_int32), ("orientation", ctypes.c_int32),
     ]
 
 
@@ -46,6 +50,7 @@ class _Lattice(ctypes.Structure):
         ("q", ctypes.c_int32), ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
         ("nz", ctypes.c_int32), ("periodic", ctypes.c_int32 * 3), ("n_dyn", ctypes.c_int32),
         ("dyn_id", ctypes.c_void_p), ("table", ctypes.POINTER(_Dyn)),
+        ("bc_values", ctypes.c_void_p),
     ]
 
 
@@ -64,6 +69,9 @@ class Dynamics:
     force: tuple = (0.0, 0.0, 0.0)
     wall_u: tuple = (0.0, 0.0, 0.0)
     wall_rho: float = 1.0
+    mixin: int = BGK          # interpolated boundaries: collision of the mixin dynamics
+    direction: int = 0        # interpolated boundaries: outward normal axis
+    orientation: int = -1     # interpolated boundaries: outward normal sign
 
 
 @dataclass
@@ -75,6 +83,7 @@ class Case:
     table: list
     dyn_id: np.ndarray | None = None  # uint8[nx*ny*nz]
     extra: dict = field(default_factory=dict)
+    bc_values: np.ndarray | None = None  # float64[4][nx*ny*nz]: RHO, VELOCITY x, y, z
 
     @property
     def n(self) -> int:
@@ -108,6 +117,9 @@ def _lattice(case: Case, keep: list):
             table[k].force[e] = d.force[e]
             table[k].wall_u[e] = d.wall_u[e]
         table[k].wall_rho = d.wall_rho
+        table[k].mixin = d.mixin
+        table[k].direction = d.direction
+        table[k].orientation = d.orientation
     lat = _Lattice()
     lat.q = case.q
     lat.nx, lat.ny, lat.nz = case.size
@@ -123,6 +135,13 @@ def _lattice(case: Case, keep: list):
         lat.dyn_id = None
     lat.table = ctypes.cast(table, ctypes.POINTER(_Dyn))
     keep.append(table)
+    if case.bc_values is not None:
+        v = np.ascontiguousarray(case.bc_values, dtype=np.float64)
+        assert v.size == 4 * case.n
+        keep.append(v)
+        lat.bc_values = v.ctypes.data
+    else:
+        lat.bc_values = None
     return lat
 
 
@@ -155,6 +174,17 @@ def step(case: Case, pops: np.ndarray, steps: int, ghost: float = float("nan"),
         return {"sum_rho": st.sum_rho, "sum_usqr": st.sum_usqr,
                 "max_usqr": st.max_usqr, "n_cells": st.n_cells}
     return None
+
+
+def post_process(case: Case, pops: np.ndarray):
+    """The PostStream post-processors alone, in place (what the reference's
+    lattice initialize() applies to the initial state)."""
+    keep: list = []
+    lat = _lattice(case, keep)
+    fn = getattr(lib(), f"oracle_post_process_{_sfx(pops.dtype)}")
+    rc = fn(ctypes.byref(lat), ctypes.c_void_p(pops.ctypes.data))
+    if rc != 0:
+        raise RuntimeError("oracle post_process failed")
 
 
 def moments(case: Case, pops: np.ndarray):
@@ -209,7 +239,8 @@ def reference_binary(q: int, dtype, variant: str = "sisd") -> Path:
 
 
 def write_case(dirpath: Path, case: Case, steps: int, init: np.ndarray | None = None,
-               rhou: np.ndarray | None = None, stats: bool = False, bench=None):
+               rhou: np.ndarray | None = None, stats: bool = False, bench=None,
+               normals: bool = False):
     """Write a case directory for olb_ref_driver (materials = dyn_id + 1)."""
     dirpath = Path(dirpath)
     dirpath.mkdir(parents=True, exist_ok=True)
@@ -217,7 +248,8 @@ def write_case(dirpath: Path, case: Case, steps: int, init: np.ndarray | None = 
     (ids.astype(np.int32) + 1).tofile(dirpath / "materials.i32")
     lines = [f"size {case.size[0]} {case.size[1]} {case.size[2]}",
              "periodic {} {} {}".format(*[int(bool(p)) for p in case.periodic])]
-    omegas = {d.omega for d in case.table if d.kind in (BGK, TRT, SMAGORINSKY, FORCED_BGK, FORCED_TRT)}
+    omegas = {d.omega for d in case.table
+              if d.kind in (BGK, TRT, SMAGORINSKY, FORCED_BGK, FORCED_TRT) + INTERPOLATED}
     if len(omegas) > 1:
         raise ValueError("the reference driver takes one lattice-wide OMEGA")
     for k, d in enumerate(case.table):
@@ -232,6 +264,18 @@ def write_case(dirpath: Path, case: Case, steps: int, init: np.ndarray | None = 
     lines.append(f"omega {ref.omega!r}")
     lines.append(f"magic {ref.magic!r}")
     lines.append(f"smagorinsky {ref.smagorinsky!r}")
+    mixins = {d.mixin for d in case.table if d.kind in INTERPOLATED}
+    if mixins:
+        if len(mixins) > 1:
+            raise ValueError("the reference driver takes one mixin dynamics for all interpolated boundaries")
+        lines.append(f"bcmixin {KIND_NAMES[mixins.pop()]}")
+        vals = case.bc_values if case.bc_values is not None else np.concatenate(
+            [np.ones(case.n), np.zeros(3 * case.n)])
+        dt = init.dtype if init is not None else rhou.dtype
+        np.ascontiguousarray(vals, dtype=dt).tofile(dirpath / "bcvalues.bin")
+        lines.append("bcvalues 1")
+    if normals:
+        lines.append(f"normals {int(normals)}")
     if init is not None:
         np.ascontiguousarray(init).tofile(dirpath / "init.bin")
         lines.append("init pops")
@@ -246,15 +290,42 @@ def write_case(dirpath: Path, case: Case, steps: int, init: np.ndarray | None = 
     (dirpath / "case.txt").write_text("\n".join(lines) + "\n")
 
 
+def reference_normals(materials: np.ndarray, periodic, boundary_materials, q: int = 19) -> np.ndarray:
+    """computeBoundaryTypeAndNormal of OpenLB itself (fluid material 1,
+    outside material 0) for every cell of `boundary_materials`: int32[4][n]
+    (type, n_x, n_y, n_z), type -1 elsewhere."""
+    m = np.ascontiguousarray(materials, dtype=np.int32)
+    size = m.shape
+    n = m.size
+    binary = reference_binary(q, np.float64)
+    with tempfile.TemporaryDirectory() as d:
+        dp = Path(d)
+        m.tofile(dp / "materials.i32")
+        lines = [f"size {size[0]} {size[1]} {size[2]}",
+                 "periodic {} {} {}".format(*[int(bool(v)) for v in periodic])]
+        for mat in sorted(int(v) for v in np.unique(m) if v != 0):
+            kind = "interpolated_velocity" if mat in boundary_materials else ("bgk" if mat == 1 else "bounce_back")
+            lines.append(f"dyn {mat} {kind}")
+        rhou = np.zeros((4, n))
+        rhou[0] = 1.0
+        rhou.tofile(dp / "rhou.bin")
+        lines += ["omega 1.0", "init eq", "steps 0", "normals 2"]
+        (dp / "case.txt").write_text("\n".join(lines) + "\n")
+        r = subprocess.run([str(binary), d], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference failed: {r.stdout[-2000:]} {r.stderr[-2000:]}")
+        return np.fromfile(dp / "out_normals.i32", dtype=np.int32).reshape(4, n)
+
+
 def run_reference(case: Case, steps: int, dtype, init: np.ndarray | None = None,
                   rhou: np.ndarray | None = None, variant: str = "sisd", stats: bool = False,
-                  threads: int | None = None):
+                  threads: int | None = None, normals: bool = False):
     """Run OpenLB itself; returns dict(pops, rho, u[, stats])."""
     binary = reference_binary(case.q, dtype, variant)
     if not binary.exists():
         raise RuntimeError(f"reference build missing: {binary} (make -C oracle/ref)")
     with tempfile.TemporaryDirectory() as d:
-        write_case(Path(d), case, steps, init=init, rhou=rhou, stats=stats)
+        write_case(Path(d), case, steps, init=init, rhou=rhou, stats=stats, normals=normals)
         env = dict(os.environ)
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
@@ -269,4 +340,6 @@ def run_reference(case: Case, steps: int, dtype, init: np.ndarray | None = None,
         }
         if stats:
             out["stats"] = np.loadtxt(Path(d) / "out_stats.txt", ndmin=2)
+        if normals:
+            out["normals"] = np.fromfile(Path(d) / "out_normals.i32", dtype=np.int32).reshape(4, n)
         return out

@@ -20,11 +20,23 @@
  *   materials.i32   int32[nx*ny*nz]
  *   init.bin        T[q][nx*ny*nz] shifted populations (f_i - w_i)   (init pops)
  *   rhou.bin        T[4][nx*ny*nz] rho, ux, uy, uz for iniEquilibrium (init eq)
+ *   bcvalues.bin    T[4][nx*ny*nz] rho, ux, uy, uz defined on the cells of
+ *                   interpolated velocity / pressure materials   (bcvalues 1)
  * Outputs written into the same directory:
  *   out_pops.bin    T[q][nx*ny*nz]   populations after `steps` collideAndStream
  *   out_rho.bin     T[nx*ny*nz]      SuperLatticeDensity3D
  *   out_u.bin       T[3][nx*ny*nz]   SuperLatticeVelocity3D
  *   out_stats.txt   one line per step: avgRho avgEnergy maxU  (when `stats 1`)
+ *   out_normals.i32 int32[4][nx*ny*nz] discrete normal type, n_x, n_y, n_z of
+ *                   every boundary-condition cell, type -1 elsewhere (`normals 1`;
+ *                   `normals 2` stops after writing it)
+ *
+ * Interpolated boundaries (`dyn <m> interpolated_velocity|interpolated_pressure`)
+ * are set like the examples do, boundary::set<InterpolatedVelocity<T,D,MIXIN>>
+ * (boundary/setBoundary.h:150-157, boundary/interpolatedVelocity3D.h:36-98),
+ * with the fluid material 1 and the outside material 0; MIXIN is the bulk
+ * dynamics named by `bcmixin`.  Their boundary values go through Cell::defineRho
+ * and Cell::defineU (core/cell.h:194-198).
  * Bench mode (`bench <warmup> <steps>` in case.txt) prints one JSON line with
  * MLUPS measured by OpenLB's own util::Timer (utilities/timer.hh:36-76).
  */
@@ -67,6 +79,9 @@ struct Case {
   bool stats = false;
   bool statisticsOn = false;
   int benchWarmup = -1, benchSteps = 0;
+  std::string bcMixin = "bgk";
+  bool bcValues = false;
+  int dumpNormals = 0;
 };
 
 Case parse_case(const std::string& dir)
@@ -95,6 +110,9 @@ Case parse_case(const std::string& dir)
     else if (key == "steps") { ls >> c.steps; }
     else if (key == "stats") { int s; ls >> s; c.stats = s; c.statisticsOn = s; }
     else if (key == "bench") { ls >> c.benchWarmup >> c.benchSteps; }
+    else if (key == "bcmixin") { ls >> c.bcMixin; }
+    else if (key == "bcvalues") { int b; ls >> b; c.bcValues = b; }
+    else if (key == "normals") { ls >> c.dumpNormals; }
     else if (key == "lattice" || key == "dtype") { /* informational, checked below */ }
     else { throw std::runtime_error("unknown key " + key); }
   }
@@ -127,6 +145,22 @@ template <typename DYN>
 void define(SuperLattice<T,DESCRIPTOR>& lattice, SuperGeometry<T,3>& geometry, int m)
 {
   lattice.template defineDynamics<DYN>(geometry, m);
+}
+
+bool is_interpolated(const std::string& kind)
+{
+  return kind == "interpolated_velocity" || kind == "interpolated_pressure";
+}
+
+template <typename MIXIN>
+void set_interpolated(SuperLattice<T,DESCRIPTOR>& lattice, SuperGeometry<T,3>& geometry, int m,
+                      const std::string& kind)
+{
+  if (kind == "interpolated_velocity") {
+    boundary::set<boundary::InterpolatedVelocity<T,DESCRIPTOR,MIXIN>>(lattice, geometry, m);
+  } else {
+    boundary::set<boundary::InterpolatedPressure<T,DESCRIPTOR,MIXIN>>(lattice, geometry, m);
+  }
 }
 
 } // namespace
@@ -176,8 +210,45 @@ int main(int argc, char* argv[])
     else if (kind == "smagorinsky") { define<SmagorinskyBGKdynamics<T,DESCRIPTOR>>(lattice, geometry, m); }
     else if (kind == "bounce_back") { define<BounceBack<T,DESCRIPTOR>>(lattice, geometry, m); }
     else if (kind == "bounce_back_velocity") { define<BounceBackVelocity<T,DESCRIPTOR>>(lattice, geometry, m); }
-    else if (kind == "none") { }
+    else if (kind == "none" || is_interpolated(kind)) { }
     else { throw std::runtime_error("unknown dynamics " + kind); }
+  }
+  if (cs.dumpNormals) {
+    auto& bg = geometry.getBlockGeometry(0);
+    BlockIndicatorMaterial3D<T> fluidI(bg, 1);
+    BlockIndicatorMaterial3D<T> outsideI(bg, 0);
+    auto materials = read_array<std::int32_t>(dir + "/materials.i32", n);
+    std::vector<std::int32_t> normals(4 * n, 0);
+    for (int x = 0; x < nx; ++x) {
+      for (int y = 0; y < ny; ++y) {
+        for (int z = 0; z < nz; ++z) {
+          const std::size_t i = (std::size_t(x) * ny + y) * nz + z;
+          normals[i] = -1;
+          auto it = cs.dyn.find(materials[i]);
+          if (it == cs.dyn.end() || !is_interpolated(it->second)) {
+            continue;
+          }
+          const auto [type, normal] = computeBoundaryTypeAndNormal(fluidI, outsideI, {x, y, z});
+          normals[i] = static_cast<std::int32_t>(type);
+          for (int d = 0; d < 3; ++d) {
+            normals[(d + 1) * n + i] = normal[d];
+          }
+        }
+      }
+    }
+    write_array(dir + "/out_normals.i32", normals);
+    if (cs.dumpNormals == 2) {
+      return 0;  // classification only
+    }
+  }
+  for (auto& [m, kind] : cs.dyn) {
+    if (!is_interpolated(kind)) {
+      continue;
+    }
+    if (cs.bcMixin == "bgk") { set_interpolated<BGKdynamics<T,DESCRIPTOR>>(lattice, geometry, m, kind); }
+    else if (cs.bcMixin == "trt") { set_interpolated<TRTdynamics<T,DESCRIPTOR>>(lattice, geometry, m, kind); }
+    else if (cs.bcMixin == "smagorinsky") { set_interpolated<SmagorinskyBGKdynamics<T,DESCRIPTOR>>(lattice, geometry, m, kind); }
+    else { throw std::runtime_error("unknown bcmixin " + cs.bcMixin); }
   }
 
   lattice.template setParameter<descriptors::OMEGA>(T(cs.omega));
@@ -228,6 +299,29 @@ int main(int argc, char* argv[])
   for (auto& [m, u] : cs.vel) {
     AnalyticalConst3D<T,T> uF(std::vector<T>{T(u[0]), T(u[1]), T(u[2])});
     lattice.defineU(geometry, m, uF);
+  }
+
+  // Boundary values of interpolated velocity / pressure cells: RHO (fixed
+  // density of pressure cells) and VELOCITY, per cell.
+  if (cs.bcValues) {
+    auto materials = read_array<std::int32_t>(dir + "/materials.i32", n);
+    auto values = read_array<T>(dir + "/bcvalues.bin", 4 * n);
+    auto& block = lattice.getBlock(0);
+    for (int x = 0; x < nx; ++x) {
+      for (int y = 0; y < ny; ++y) {
+        for (int z = 0; z < nz; ++z) {
+          const std::size_t i = (std::size_t(x) * ny + y) * nz + z;
+          auto it = cs.dyn.find(materials[i]);
+          if (it == cs.dyn.end() || !is_interpolated(it->second)) {
+            continue;
+          }
+          auto cell = block.get({x, y, z});
+          T u[3] = {values[n + i], values[2 * n + i], values[3 * n + i]};
+          cell.defineRho(values[i]);
+          cell.defineU(u);
+        }
+      }
+    }
   }
 
   lattice.initialize();

@@ -96,14 +96,59 @@ def channel_cylinder_case(q, size, omega=1.6, smagorinsky=0.1, side=4):
                          O.Dynamics(O.BOUNCE_BACK)])
 
 
+def interpolated_channel_case(q, size, mixin=O.BGK, omega=1.6, smagorinsky=0.1, magic=3 / 16,
+                              u0=0.05, fluctuation=0.02, rho_out=1.0, side=0, seed=0):
+    """Channel with bounce-back walls on the y/z faces, an interpolated
+    velocity inlet on the x = 0 face and an interpolated pressure outlet on the
+    x = nx-1 face (both over the interior y/z cells, so every boundary cell is a
+    flat one), optionally a square cylinder spanning z.  The inlet velocity is
+    u0 along x with seeded uniform fluctuations of relative size
+    `fluctuation` on every component; the outlet holds rho_out.
+    Ids: 0 fluid, 1 wall, 2 inlet (normal -x), 3 outlet (normal +x)."""
+    nx, ny, nz = size
+    ids = np.zeros(size, np.uint8)
+    ids[:, 0, :] = ids[:, -1, :] = 1
+    ids[:, :, 0] = ids[:, :, -1] = 1
+    ids[0, 1:-1, 1:-1] = 2
+    ids[-1, 1:-1, 1:-1] = 3
+    if side:
+        x0, y0 = nx // 4, ny // 2 - side // 2
+        ids[x0:x0 + side, y0:y0 + side, 1:-1] = 1
+    rng = np.random.default_rng(seed)
+    vals = np.zeros((4,) + tuple(size))
+    vals[0] = 1.0
+    r = 2 * rng.random((3, ny, nz)) - 1
+    vals[1, 0] = u0 * (1 + fluctuation * r[0])
+    vals[2, 0] = u0 * fluctuation * r[1]
+    vals[3, 0] = u0 * fluctuation * r[2]
+    vals[0, -1] = rho_out
+    bulk = dict(omega=omega, magic=magic, smagorinsky=smagorinsky)
+    table = [O.Dynamics(mixin, **bulk), O.Dynamics(O.BOUNCE_BACK),
+             O.Dynamics(O.INTERP_VELOCITY, mixin=mixin, direction=0, orientation=-1, **bulk),
+             O.Dynamics(O.INTERP_PRESSURE, mixin=mixin, direction=0, orientation=1, **bulk)]
+    return O.Case(q=q, size=size, periodic=(0, 0, 0), dyn_id=ids.reshape(-1), table=table,
+                  bc_values=vals.reshape(4, -1))
+
+
 def to_abi_table(case):
     """oracle.Case -> openlb_b200 dynamics table (same entries, same ids)."""
     import openlb_b200 as ob
     table = []
     for d in case.table:
+        extra = {}
+        if d.kind in O.INTERPOLATED:
+            extra = dict(mixin=d.mixin, direction=d.direction, orientation=d.orientation)
         table.append(ob.Dynamics(kind=d.kind, omega=d.omega, magic=d.magic, smagorinsky=d.smagorinsky,
-                                 force=tuple(d.force), wall_u=tuple(d.wall_u), wall_rho=d.wall_rho))
+                                 force=tuple(d.force), wall_u=tuple(d.wall_u), wall_rho=d.wall_rho, **extra))
     return table
+
+
+def boundary_cells_and_values(case):
+    """(cells, values[k, 4]) of the interpolated boundary cells of a case, for
+    Lattice.set_boundary_values."""
+    kinds = np.array([d.kind for d in case.table])
+    cells = np.flatnonzero(np.isin(kinds[case.dyn_id], O.INTERPOLATED))
+    return cells, case.bc_values[:, cells].T.copy()
 
 
 def pop_tolerance_violation(q, got, ref, rtol, dtype=np.float64):

@@ -6,7 +6,8 @@ Each fixture is the output of the reference's own CPU_SISD build
 sources with OpenLB's public API) on a small seeded case: the inputs (geometry
 ids, dynamics table, initial populations) and the reference's populations,
 Density3D / Velocity3D fields and per-step LatticeStatistics after the stated
-number of collideAndStream steps.
+number of collideAndStream steps (after the lattice's initialize(), which
+applies the PostStream post-processors once to the initial state).
 
     python tests/golden/make_golden.py        # needs oracle/_ref (make -C oracle/ref)
 
@@ -64,23 +65,80 @@ def fixture_cases():
     u[0] = 0.05
     f0 = O.equilibrium(27, np.ones(n, np.float32), u)
     out.append(("channel_q27_float32_sisd", case, f0, 10, np.float32, "sisd", True))
+    # interpolated velocity inlet / pressure outlet (PlaneFdBoundaryProcessor3D)
+    for q, dtype, mixin, side in ((19, np.float32, O.BGK, 0), (19, np.float64, O.BGK, 2),
+                                  (19, np.float64, O.TRT, 0), (27, np.float32, O.SMAGORINSKY, 2),
+                                  (27, np.float64, O.SMAGORINSKY, 0)):
+        case = C.interpolated_channel_case(q, (12, 8, 7), mixin=mixin, side=side, seed=q + side)
+        f0 = C.rest_state(q, case.n, dtype)
+        name = f"interp_channel_q{q}_{np.dtype(dtype).name}_{O.KIND_NAMES[mixin]}_sisd"
+        out.append((name, case, f0, 30, dtype, "sisd", True))
+    return out
+
+
+def normals_geometries():
+    """Material layouts whose boundary cells (material 3) cover flat faces,
+    edges and corners; fluid is material 1, walls 2, outside 0."""
+    out = []
+    # channel with inlet/outlet planes bounded by walls and a square cylinder
+    case = C.interpolated_channel_case(19, (12, 8, 7), side=2)
+    mats = case.dyn_id.reshape(case.size).astype(np.int32) + 1
+    mats[mats == 4] = 3
+    out.append(("normals_channel", mats, (0, 0, 0)))
+    # inlet spanning the whole x = 0 face (its rim touches the outside), x periodic
+    mats = np.full((9, 8, 7), 1, np.int32)
+    mats[:, 0, :] = mats[:, -1, :] = 2
+    mats[0, :, :] = 3
+    out.append(("normals_open_face", mats, (0, 0, 1)))
+    # random fluid boxes in a wall block, boundary cells sampled next to fluid,
+    # an outside pocket
+    rng = np.random.default_rng(11)
+    for k in range(3):
+        size = (14, 12, 10)
+        mats = np.full(size, 2, np.int32)
+        for _ in range(4):
+            lo = rng.integers(1, np.array(size) - 4)
+            hi = np.minimum(lo + rng.integers(3, 7, 3), np.array(size) - 1)
+            mats[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = 1
+        fluid = mats == 1
+        near = np.zeros(size, bool)
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    near |= np.roll(fluid, (dx, dy, dz), axis=(0, 1, 2))
+        cand = near & ~fluid
+        mats[cand & (rng.random(size) < 0.7)] = 3
+        mats[-3:, -3:, :] = np.where(mats[-3:, -3:, :] == 1, 1, 0)
+        out.append((f"normals_random{k}", mats, (0, 0, 0)))
     return out
 
 
 def main():
     manifest = {}
+    for name, mats, periodic in normals_geometries():
+        ref = O.reference_normals(mats, periodic, boundary_materials=(3,))
+        path = HERE / f"{name}.npz"
+        np.savez_compressed(path, materials=mats, periodic=np.array(periodic, np.int32), normals=ref)
+        manifest[name] = {"variant": "sisd", "dtype": "int32", "steps": 0,
+                          "sha256": hashlib.sha256(path.read_bytes()).hexdigest()}
+        print(name, path.stat().st_size, "types", np.unique(ref[0][ref[0] >= 0], return_counts=True))
     for name, case, f0, steps, dtype, variant, stats in fixture_cases():
-        ref = O.run_reference(case, steps, dtype, init=f0, variant=variant, stats=stats)
+        # one thread: the reference applies post-processors in an OpenMP loop
+        # in place, so neighbouring pressure-boundary cells race otherwise
+        ref = O.run_reference(case, steps, dtype, init=f0, variant=variant, stats=stats, threads=1)
         payload = {
             "q": np.int32(case.q), "size": np.array(case.size, np.int32),
             "periodic": np.array(case.periodic, np.int32), "steps": np.int32(steps),
             "dyn_id": case.dyn_id if case.dyn_id is not None else np.zeros(case.n, np.uint8),
-            "table": np.array([[d.kind, d.omega, d.magic, d.smagorinsky, *d.force, *d.wall_u, d.wall_rho]
+            "table": np.array([[d.kind, d.omega, d.magic, d.smagorinsky, *d.force, *d.wall_u, d.wall_rho,
+                                d.mixin, d.direction, d.orientation]
                                for d in case.table], np.float64),
             "init": f0, "pops": ref["pops"], "rho": ref["rho"], "u": ref["u"],
         }
         if stats:
             payload["stats"] = ref["stats"]
+        if case.bc_values is not None:
+            payload["bc_values"] = case.bc_values
         path = HERE / f"{name}.npz"
         np.savez_compressed(path, **payload)
         manifest[name] = {"variant": variant, "dtype": np.dtype(dtype).name, "steps": steps,
@@ -90,6 +148,7 @@ def main():
     (HERE / "MANIFEST.json").write_text(json.dumps(
         {"generator": "tests/golden/make_golden.py", "reference_build": "oracle/ref/Makefile",
          "compiler": gxx, "flags": "-O3 -std=c++20 -march=x86-64-v2 -ffp-contract=off -fopenmp",
+         "threads": 1,
          "fixtures": manifest}, indent=1) + "\n")
 
 

@@ -10,6 +10,14 @@ collision templates operation for operation, so:
     population for FP32, 1e-13 for FP64.
 Slots the oracle marks NaN depend on OpenLB's unspecified padding and are not
 compared (they never reach a fluid cell).
+
+Every run starts like the reference's lattice.initialize(): the PostStream
+post-processors are applied once to the initial state.  The interpolated
+boundary fixtures (interp_channel_*) are compared to rounding: the reference's
+D3Q19 boundary collisions are CSE-generated, and its post-processor visits
+boundary cells in place one after the other, while the oracle evaluates every
+boundary cell from the post-stream state (the two differ by rounding, because
+regularisation keeps a cell's density and momentum).
 """
 import json
 from pathlib import Path
@@ -20,19 +28,32 @@ import pytest
 from oracle import oracle as O
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-FIXTURES = sorted(p.stem for p in GOLDEN.glob("*.npz"))
+FIXTURES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("normals_"))
 
 
 def load(name):
     z = np.load(GOLDEN / f"{name}.npz")
     table = [O.Dynamics(int(r[0]), omega=r[1], magic=r[2], smagorinsky=r[3], force=tuple(r[4:7]),
-                        wall_u=tuple(r[7:10]), wall_rho=r[10]) for r in z["table"]]
+                        wall_u=tuple(r[7:10]), wall_rho=r[10], mixin=int(r[11]), direction=int(r[12]),
+                        orientation=int(r[13])) for r in z["table"]]
     case = O.Case(q=int(z["q"]), size=tuple(int(s) for s in z["size"]),
-                  periodic=tuple(int(p) for p in z["periodic"]), table=table, dyn_id=z["dyn_id"])
+                  periodic=tuple(int(p) for p in z["periodic"]), table=table, dyn_id=z["dyn_id"],
+                  bc_values=z["bc_values"] if "bc_values" in z.files else None)
     return z, case
 
 
+def run_oracle(z, case, steps):
+    """initialize() (PostStream post-processors on the initial state), then steps."""
+    f = z["init"].copy()
+    O.post_process(case, f)
+    if steps:
+        O.step(case, f, steps)
+    return f
+
+
 def expected_exact(name):
+    if name.startswith("interp_"):
+        return False
     if name.endswith("_nocse") or "_q27_" in name:
         return True
     # D3Q19 CSE specialisations exist for BGK and Smagorinsky-BGK
@@ -41,15 +62,14 @@ def expected_exact(name):
 
 def test_fixture_inventory():
     manifest = json.loads((GOLDEN / "MANIFEST.json").read_text())
-    assert set(manifest["fixtures"]) == set(FIXTURES)
+    assert set(manifest["fixtures"]) == {p.stem for p in GOLDEN.glob("*.npz")}
     assert len(FIXTURES) >= 25
 
 
 @pytest.mark.parametrize("name", FIXTURES)
 def test_oracle_matches_reference(name):
     z, case = load(name)
-    f = z["init"].copy()
-    O.step(case, f, int(z["steps"]))
+    f = run_oracle(z, case, int(z["steps"]))
     ref = z["pops"]
     valid = ~np.isnan(f)
     assert valid.mean() > 0.6
@@ -62,14 +82,17 @@ def test_oracle_matches_reference(name):
         # 0.0555555555555556 for 1/18), so in FP64 the reference's own two
         # paths differ by more than one rounding: ~2e-10 for Smagorinsky
         tol = 2e-6 if f.dtype == np.float32 else 1e-9
+        if name.startswith("interp_") and f.dtype == np.float32:
+            # finite-difference velocity gradients of the boundary cells
+            # amplify the rounding differences of the D3Q19 CSE collisions
+            tol = 1e-5
         assert rel.max() <= tol, (name, rel.max())
 
 
 @pytest.mark.parametrize("name", FIXTURES)
 def test_oracle_moments_match_reference_functors(name):
     z, case = load(name)
-    f = z["init"].copy()
-    O.step(case, f, int(z["steps"]))
+    f = run_oracle(z, case, int(z["steps"]))
     valid_cell = ~np.isnan(f.reshape(case.q, -1)).any(axis=0)
     rho, u = O.moments(case, np.where(np.isnan(f), 0, f).astype(f.dtype))
     ids = case.dyn_id
@@ -80,13 +103,12 @@ def test_oracle_moments_match_reference_functors(name):
     np.testing.assert_allclose(u[:, check], z["u"][:, check], rtol=0, atol=tol)
 
 
-@pytest.mark.parametrize("name", [n for n in FIXTURES if n.startswith(("cavity", "porous", "channel"))])
+@pytest.mark.parametrize("name", [n for n in FIXTURES if n.startswith(("cavity", "porous", "channel", "interp"))])
 def test_oracle_statistics_match_reference(name):
     """LatticeStatistics of the last step: avg rho, avg energy, max |u|^2."""
     z, case = load(name)
-    f = z["init"].copy()
     steps = int(z["steps"])
-    O.step(case, f, steps - 1)
+    f = run_oracle(z, case, steps - 1)
     st = O.step(case, f, 1, with_stats=True)
     avg_rho, avg_energy, max_u = z["stats"][-1]
     n = st["n_cells"]
