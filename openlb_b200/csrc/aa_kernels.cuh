@@ -293,8 +293,10 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict
         counted = true;
       }
     }
-    // NoDynamics (and anything else): populations pass through unchanged
-    Neighbours nb(g, x, y, z);
+    // NoDynamics (and anything else): populations pass through unchanged.
+    // The store offsets are recomputed here rather than kept live through
+    // the collision.
+    Neighbours nb(g, int(opaque(uint32_t(x))), int(opaque(uint32_t(y))), int(opaque(uint32_t(z))));
     const uint32_t stride = opaque(g.stride);
     const uint32_t nk = opaque(n[k]);
     static_for<0, Q>([&](auto i) {
@@ -345,6 +347,21 @@ template <> struct Pair<__nv_bfloat16> {
   OLB_DEV static float2 to_float2(T v) { return __bfloat1622float2(v); }
   OLB_DEV static T from_floats(float lo, float hi) { return __floats2bfloat162_rn(lo, hi); }
 };
+
+// byte permutation of a packed pair (one PRMT): 0x3210 keeps it, 0x1032 swaps
+// the halves; pair_merge_lo/hi take the low/high halves of a and b
+template <class T>
+OLB_DEV T pair_perm(T a, T b, uint32_t sel)
+{
+  static_assert(sizeof(T) == 4, "packed 16-bit pair");
+  uint32_t ua, ub;
+  memcpy(&ua, &a, 4);
+  memcpy(&ub, &b, 4);
+  const uint32_t r = __byte_perm(ua, ub, sel);
+  T out;
+  memcpy(&out, &r, 4);
+  return out;
+}
 
 struct PairNeighbours {
   uint32_t xo[3], yo[3], zo[3];
@@ -470,9 +487,8 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
           constexpr int o = L::opp(i);
           const uint32_t src = nb.template at<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>();
           const T v = pops[size_t(o) * pstride + src];
-          if (nb.swap[1 - L::c(i, 0)]) {
-            raw[k][i].x = v.y;
-            raw[k][i].y = v.x;
+          if constexpr (L::c(i, 0) != 0) {
+            raw[k][i] = pair_perm(v, v, nb.swap[1 - L::c(i, 0)] ? 0x1032u : 0x3210u);
           } else {
             raw[k][i] = v;
           }
@@ -484,38 +500,67 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
   static_for<0, CPT>([&](auto k) {
     if (!go[k]) return;
     const int y = y0 + k.value * int(blockDim.y);
-    // in the odd step the value read for population i is column opp(i)'s storage
-    auto unpack = [&](auto half_tag) {
-      float f[Q];
-      static_for<0, Q>([&](auto i) {
-        constexpr int col = ODD ? L::opp(i) : i.value;
-        constexpr float inv = 1.f / storage_scale<L>(col);
-        const float2 fv = P::to_float2(raw[k][i]);
-        f[i] = (decltype(half_tag)::value ? fv.y : fv.x) * inv;
-      });
-      return f;
-    };
+    // Both cells of the pair are collided in the scaled representation
+    // g_i = s_i (f_i - w_i) of the storage, one after the other.  BGK and
+    // TRT cells collide on g directly (relax_*_scaled); any other dynamics
+    // decodes f_i = g_i / s_i, collides and re-encodes.  s_i of a population
+    // equals that of its opposite, so the column read or written (i or
+    // opp(i)) does not change the scale.
+    // the low cell's results wait in packed pairs of populations (half the
+    // registers); the high cell's are packed the same way and the two are
+    // merged with one byte permutation per population
+    constexpr int QP = (Q + 1) / 2;
+    T lo_pack[QP];
     auto cell = [&](auto half_tag, int kind, const DynDevice<float>* pe) {
       constexpr bool HI = decltype(half_tag)::value;
       const int x = HI ? xp + (g.nx >> 1) : xp;
-      float f[Q];
+      float gout[Q];
       static_for<0, Q>([&](auto i) {
-        constexpr int col = ODD ? L::opp(i) : i.value;
-        constexpr float inv = 1.f / storage_scale<L>(col);
         const float2 fv = P::to_float2(raw[k][i]);
-        f[i] = (HI ? fv.y : fv.x) * inv;
+        gout[i] = HI ? fv.y : fv.x;
       });
       float r = 0.f, u2 = 0.f;
-      const bool counted = collide_any<L, KIND, MASKED>(f, kind, pe, bulk, x, y, z, r, u2);
-      // repack: the written value is population i in column (ODD ? i : opp(i))
-      static_for<0, Q>([&](auto i) {
-        constexpr int col = ODD ? i.value : L::opp(i);
-        constexpr float sc = storage_scale<L>(col);
-        const T packed = P::from_floats(f[i] * sc, f[i] * sc);
-        if constexpr (HI) {
-          raw[k][i].y = packed.y;
+      bool counted = false, done = false;
+#ifndef OLB_B200_EXACT
+      if constexpr (KIND == K_BGK || KIND == K_TRT) {
+        if (!MASKED || kind == KIND) {
+          float rho, u[3];
+          scaled_rho_u<L>(gout, rho, u);
+          const float om = MASKED ? __ldg(&pe->omega) : bulk.omega;
+          if constexpr (KIND == K_TRT) {
+            relax_trt_scaled<L>(gout, rho, u, om, MASKED ? __ldg(&pe->omega_minus) : bulk.omega_minus);
+          } else {
+            relax_bgk_scaled<L>(gout, rho, u, om);
+          }
+          r = rho;
+          u2 = norm_sqr(u);
+          counted = true;
+          done = true;
+        }
+      }
+#endif
+      if (!done) {
+        static_for<0, Q>([&](auto i) {
+          constexpr float inv = 1.f / storage_scale<L>(i);
+          gout[i] *= inv;
+        });
+        counted = collide_any<L, KIND, MASKED>(gout, kind, pe, bulk, x, y, z, r, u2);
+        static_for<0, Q>([&](auto i) {
+          constexpr float sc = storage_scale<L>(i);
+          gout[i] *= sc;
+        });
+      }
+      static_for<0, QP>([&](auto jj) {
+        constexpr int a = 2 * jj.value;
+        constexpr int b = a + 1 < Q ? a + 1 : a;
+        const T packed = P::from_floats(gout[a], gout[b]);
+        if constexpr (!HI) {
+          lo_pack[jj] = packed;
         } else {
-          raw[k][i].x = packed.x;
+          raw[k][a] = pair_perm(lo_pack[jj], packed, 0x5410u);
+          if constexpr (a + 1 < Q) {
+            raw[k][a + 1] = pair_perm(lo_pack[jj], packed, 0x7632u);
+          }
         }
       });
       if constexpr (STATS) {
@@ -526,10 +571,10 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
         }
       }
     };
-    (void)unpack;
     cell(std::integral_constant<bool, false>{}, kind_lo[k], p_lo[k]);
     cell(std::integral_constant<bool, true>{}, kind_hi[k], p_hi[k]);
-    PairNeighbours nb(g, xp, y, z);
+    // recomputed after the collision rather than kept live through it
+    PairNeighbours nb(g, int(opaque(uint32_t(xp))), int(opaque(uint32_t(y))), int(opaque(uint32_t(z))));
     const uint32_t ps = opaque(pstride);
     const uint32_t ek = opaque(e[k]);
     static_for<0, Q>([&](auto i) {
@@ -539,9 +584,8 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
       } else {
         const uint32_t dst = nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>();
         T v = raw[k][i];
-        if (nb.swap[1 + L::c(i, 0)]) {
-          v.x = raw[k][i].y;
-          v.y = raw[k][i].x;
+        if constexpr (L::c(i, 0) != 0) {
+          v = pair_perm(v, v, nb.swap[1 + L::c(i, 0)] ? 0x1032u : 0x3210u);
         }
         pops[size_t(i.value) * ps + dst] = v;
       }

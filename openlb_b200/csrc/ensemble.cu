@@ -4,9 +4,9 @@
 // All admitted instances live in one device pool.  Each instance owns a region
 // holding its q population columns (AA layout, as a single lattice) and three
 // columns with the velocity of its last convergence check.  One kernel launch
-// advances every active instance by one step: a fixed grid of blocks walks a
-// tile list, each tile being 256 x kTileCells consecutive cells of one
-// instance's flattened cell index (z fastest).  Cell coordinates come from the
+// advances every active instance by one step: one block per tile of a tile
+// list, each tile being 256 x kTileCells consecutive cells of one instance's
+// flattened cell index (z fastest).  Cell coordinates come from the
 // flat index by multiply-shift division (Granlund & Montgomery, "Division by
 // invariant integers using multiplication", PLDI 1994) with per-instance
 // constants, so instances of any size share the launch without idle lanes.
@@ -18,9 +18,10 @@
 // instance in a fixed order, so results do not depend on the mix), in a pass
 // over the logical post-stream state after the chunk.
 //
-// The grid and the kernel arguments never change while instances come and go
-// (the host rewrites the tables in device memory), so a chunk of steps is
-// captured once as a CUDA graph and replayed.
+// The kernel arguments never change while instances come and go (the host
+// rewrites the tables in device memory) and the step grid is the tile count
+// rounded up by at most 25 %, so a chunk of steps is captured once as a CUDA
+// graph and replayed until the load changes notably.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,7 +46,7 @@ namespace {
 constexpr int kQ = 19;
 using L19 = Lattice<19>;
 constexpr int kEnsembleThreads = 256;
-constexpr int kTileCells = 2;  // cells per thread in a tile
+constexpr int kTileCells = 1;  // cells per thread in a tile
 constexpr int kTile = kEnsembleThreads * kTileCells;
 
 // q = floor(n / d) for n < 2^31 by one multiply-high, an add and a shift
@@ -340,8 +341,9 @@ struct olb_b200_ensemble {
   float* moments_dev = nullptr;                // staging for get_moments
   size_t moments_cap = 0;
   bool dirty = true;                           // tables changed since upload
-  int grid = 0;
-  int min_blocks = 3;
+  int grid = 0;                                // persistent grid of the check kernel
+  int step_grid = 0;                           // blocks of the step kernel: ntiles rounded up
+  int min_blocks = 4;
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -437,6 +439,24 @@ olb_b200_status upload_tables(olb_b200_ensemble* E)
     OLB_ECUDA(cudaMalloc(&E->partials, size_t(cap) * sizeof(ResidualPartial)));
     E->max_tiles = cap;
   }
+  // one block per tile, the grid rounded up (at most 25 %) so that it, and
+  // with it the captured graph, only changes when the load changes notably;
+  // blocks past the tile count return at once
+  {
+    const int n = std::max(1, int(tiles.size()));
+    int p = 1;
+    while (p * 2 <= n) p *= 2;
+    const int quantum = std::max(1, p / 4);
+    const int bucket = (n + quantum - 1) / quantum * quantum;
+    if (bucket != E->step_grid) {
+      if (E->graph) {
+        OLB_ECUDA(cudaStreamSynchronize(E->stream));
+        cudaGraphExecDestroy(E->graph);
+        E->graph = nullptr;
+      }
+      E->step_grid = bucket;
+    }
+  }
   const int counts[2] = {int(tiles.size()), E->max_instances};
   if (!tiles.empty()) {
     OLB_ECUDA(cudaMemcpyAsync(E->tiles_dev, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice, E->stream));
@@ -457,15 +477,15 @@ olb_b200_status enqueue_chunk(olb_b200_ensemble* E, int steps, int check)
   for (int k = 0; k < steps; ++k) {
     switch (E->min_blocks) {
     case 2:
-      ensemble_step_kernel<2><<<E->grid, kEnsembleThreads, 0, E->stream>>>(
+      ensemble_step_kernel<2><<<E->step_grid, kEnsembleThreads, 0, E->stream>>>(
         E->pool, E->table_dev, E->tiles_dev, E->counts_dev, k);
       break;
     case 4:
-      ensemble_step_kernel<4><<<E->grid, kEnsembleThreads, 0, E->stream>>>(
+      ensemble_step_kernel<4><<<E->step_grid, kEnsembleThreads, 0, E->stream>>>(
         E->pool, E->table_dev, E->tiles_dev, E->counts_dev, k);
       break;
     default:
-      ensemble_step_kernel<3><<<E->grid, kEnsembleThreads, 0, E->stream>>>(
+      ensemble_step_kernel<3><<<E->step_grid, kEnsembleThreads, 0, E->stream>>>(
         E->pool, E->table_dev, E->tiles_dev, E->counts_dev, k);
       break;
     }
@@ -535,7 +555,7 @@ olb_b200_status olb_b200_ensemble_create(const olb_b200_ensemble_desc* desc, olb
   OLB_ECUDA_C(cudaMemsetAsync(E->steps_dev, 0, size_t(E->max_instances) * sizeof(uint32_t), E->stream));
   int sms = 0;
   OLB_ECUDA_C(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E->device));
-  E->min_blocks = 3;
+  E->min_blocks = 4;
   E->grid = sms * E->min_blocks;
   olb_b200_status st = upload_tables(E);
   if (st != OLB_B200_OK) return cleanup(st);

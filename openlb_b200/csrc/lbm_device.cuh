@@ -532,6 +532,118 @@ OLB_DEV void collide_interpolated(R (&f)[L::q], int kind, const DynDevice<R>* __
   st_usqr = norm_sqr(u);
 }
 
+// ---------------------------------------------------------------------------
+// BGK / TRT on the scaled 16-bit representation g_i = s_i (f_i - w_i)
+//
+// 16-bit storage keeps s_i (f_i - w_i), s_i a power of two that depends only
+// on the weight class |c_i|^2.  Decoding every population (g_i / s_i) and
+// encoding the result (s_i f_i') costs two multiplies per population.  On g
+// directly the moments need one multiply per weight class and the relaxation
+// none, g_i' = (1 - omega) g_i + omega s_i feq_i, with s_i t_i folded into the
+// equilibrium's constants.  Algebraically the same collision; the rounding
+// differs well below the 16-bit storage's own.
+
+template <class L>
+OLB_HD constexpr int weight_class(int i)
+{
+  return L::c(i, 0) * L::c(i, 0) + L::c(i, 1) * L::c(i, 1) + L::c(i, 2) * L::c(i, 2);
+}
+
+template <class L>
+OLB_HD constexpr int first_of_class(int k)
+{
+  int i = 0;
+  while (i < L::q && weight_class<L>(i) != k) ++i;
+  return i;
+}
+
+template <class L>
+OLB_HD constexpr float inv_class_scale(int k)
+{
+  return first_of_class<L>(k) < L::q ? 1.f / storage_scale<L>(first_of_class<L>(k)) : 0.f;
+}
+
+template <class L>
+OLB_DEV void scaled_rho_u(const float (&g)[L::q], float& rho, float (&u)[3])
+{
+  float m[4] = {0.f, 0.f, 0.f, 0.f};
+  float j[3][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+  static_for<0, L::q>([&](auto i) {
+    constexpr int k = weight_class<L>(i);
+    m[k] += g[i];
+    static_for<0, 3>([&](auto d) {
+      constexpr int cc = L::c(i, d);
+      if constexpr (cc == 1) { j[d][k] += g[i]; }
+      else if constexpr (cc == -1) { j[d][k] -= g[i]; }
+    });
+  });
+  rho = 1.f;
+  u[0] = u[1] = u[2] = 0.f;
+  static_for<0, 4>([&](auto k) {
+    constexpr float inv = inv_class_scale<L>(k);
+    if constexpr (inv != 0.f) {
+      rho += m[k] * inv;
+      u[0] += j[0][k] * inv;
+      u[1] += j[1][k] * inv;
+      u[2] += j[2][k] * inv;
+    }
+  });
+  const float r = 1.f / rho;
+  u[0] *= r; u[1] *= r; u[2] *= r;
+}
+
+// BGK (pair form) on g, with omega folded into the equilibrium terms:
+// g_i' = (1 - omega) g_i + A + B, g_opp' = (1 - omega) g_opp + A - B,
+// A = omega s t (rho (1 + 9/2 (c.u)^2 - 3/2 |u|^2) - 1), B = 3 omega s t rho (c.u)
+template <class L>
+OLB_DEV void relax_bgk_scaled(float (&g)[L::q], float rho, const float (&u)[3], float omega)
+{
+  const float usqr = norm_sqr(u);
+  const float even0 = 1.f - 1.5f * usqr;
+  const float keep = 1.f - omega;
+  {
+    constexpr float T = storage_scale<L>(0) * weight<L, float>(0);
+    const float wt = omega * T;
+    g[0] = keep * g[0] + ((rho * wt) * even0 - wt);
+  }
+  static_for<1, L::half + 1>([&](auto i) {
+    constexpr int o = L::opp(i);
+    constexpr float T = storage_scale<L>(i) * weight<L, float>(i);
+    const float wt = omega * T;
+    const float rwt = rho * wt;
+    const float cu = c_dot<L, i.value>(u);
+    const float a = rwt * (even0 + 4.5f * cu * cu) - wt;
+    const float b = (rwt * 3.f) * cu;
+    g[i] = (keep * g[i] + a) + b;
+    g[o] = (keep * g[o] + a) - b;
+  });
+}
+
+template <class L>
+OLB_DEV void relax_trt_scaled(float (&g)[L::q], float rho, const float (&u)[3], float omega, float omega_minus)
+{
+  const float usqr = norm_sqr(u);
+  const float even0 = 1.f - 1.5f * usqr;
+  {
+    constexpr float T = storage_scale<L>(0) * weight<L, float>(0);
+    g[0] -= omega * (g[0] - (rho * T * even0 - T));
+  }
+  static_for<1, L::half + 1>([&](auto i) {
+    constexpr int o = L::opp(i);
+    constexpr float T = storage_scale<L>(i) * weight<L, float>(i);
+    const float rt = rho * T;
+    const float cu = c_dot<L, i.value>(u);
+    const float a = rt * (even0 + 4.5f * cu * cu) - T;
+    const float b = (rt * 3.f) * cu;
+    const float dp = omega * (0.5f * (g[i] + g[o]) - a);
+    const float dm = omega_minus * (0.5f * (g[i] - g[o]) - b);
+    const float gi = g[i] - dp - dm;
+    const float go = g[o] - dp + dm;
+    g[i] = gi;
+    g[o] = go;
+  });
+}
+
 // collision::NguyenLaddCorrection<Revert>  src/dynamics/collision.h:333-346
 template <class L, class R>
 OLB_DEV void collide_moving_wall(R (&f)[L::q], const DynDevice<R>& p)

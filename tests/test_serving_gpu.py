@@ -134,10 +134,11 @@ def test_slot_limit():
         ens.close()
 
 
-def test_batched_and_plain_loops_agree():
+@pytest.mark.parametrize("style", ["chunked", "per_step"])
+def test_batched_and_plain_loops_agree(style):
     reqs = serving.make_requests(8, rate=0.0, seed=11, n_range=(16, 30), tol=1e-4, max_steps=600)
     b = serving.serve_batched(reqs, 1 << 30, 16, check_interval=100, keep_velocity=True)
-    p = serving.serve_plain(reqs, check_interval=100, keep_velocity=True)
+    p = serving.serve_plain(reqs, check_interval=100, keep_velocity=True, style=style)
     assert b["solves"] == p["solves"] == len(reqs)
     rb = {r.rid: r for r in b["results"]}
     rp = {r.rid: r for r in p["results"]}
