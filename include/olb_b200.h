@@ -153,6 +153,18 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* lattice, const uint8_t* 
 olb_b200_status olb_b200_set_boundary_values(olb_b200_lattice* lattice, const int64_t* cells, int64_t count,
                                              const double* values);
 
+/* Per-step fluctuations of the interpolated velocity inlets — what an OpenLB
+ * example does by calling defineU with a random field before every step.  No
+ * counterpart in the reference's library.  Before step t (t = steps done so
+ * far) every interpolated-velocity cell gets
+ *   VELOCITY_d = U_d + amplitude * |U| * (2 r - 1),
+ * U the values set by olb_b200_set_boundary_values and r the top 53 bits of
+ * splitmix64(seed + (t * cells + cell) * 3 + d) over 2^53 (splitmix64 as in
+ * Steele, Lea, Flood, OOPSLA 2014: x += 0x9E3779B97F4A7C15;
+ * x = (x ^ x>>30) * 0xBF58476D1CE4E5B9; x = (x ^ x>>27) * 0x94D049BB133111EB;
+ * x ^ x>>31).  amplitude 0 turns it off and restores U.  Synchronous. */
+olb_b200_status olb_b200_set_boundary_noise(olb_b200_lattice* lattice, double amplitude, uint64_t seed);
+
 /* SuperLattice::initialize (src/core/superLattice.hh:191-204,
  * src/core/blockLattice.hh:56-67): applies the PostStream post-processors
  * (the interpolated boundaries) once to the current state.  The first

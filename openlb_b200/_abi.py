@@ -44,7 +44,7 @@ EXPORTED = [
     "olb_b200_ensemble_create", "olb_b200_ensemble_destroy", "olb_b200_ensemble_add",
     "olb_b200_ensemble_remove", "olb_b200_ensemble_run", "olb_b200_ensemble_get_moments",
     "olb_b200_ensemble_info", "olb_b200_ensemble_set_occupancy", "olb_b200_ensemble_bytes_per_instance",
-    "olb_b200_set_boundary_values", "olb_b200_initialize",
+    "olb_b200_set_boundary_values", "olb_b200_initialize", "olb_b200_set_boundary_noise",
 ]
 
 ENSEMBLE_CAVITY, ENSEMBLE_CHANNEL = 1, 2
@@ -194,6 +194,8 @@ def load(variant: str = "fast") -> ctypes.CDLL:
     lib.olb_b200_ensemble_bytes_per_instance.restype = ctypes.c_uint64
     lib.olb_b200_set_boundary_values.argtypes = [P, P, ctypes.c_int64, P]
     lib.olb_b200_set_boundary_values.restype = st
+    lib.olb_b200_set_boundary_noise.argtypes = [P, ctypes.c_double, ctypes.c_uint64]
+    lib.olb_b200_set_boundary_noise.restype = st
     lib.olb_b200_initialize.argtypes = [P]
     lib.olb_b200_initialize.restype = st
     lib.olb_b200_last_error.argtypes = []

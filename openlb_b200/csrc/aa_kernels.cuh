@@ -524,13 +524,13 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
 #ifndef OLB_B200_EXACT
       if constexpr (KIND == K_BGK || KIND == K_TRT) {
         if (!MASKED || kind == KIND) {
-          float rho, u[3];
-          scaled_rho_u<L>(gout, rho, u);
+          float rho, delta, u[3];
+          scaled_rho_u<L>(gout, rho, delta, u);
           const float om = MASKED ? __ldg(&pe->omega) : bulk.omega;
           if constexpr (KIND == K_TRT) {
-            relax_trt_scaled<L>(gout, rho, u, om, MASKED ? __ldg(&pe->omega_minus) : bulk.omega_minus);
+            relax_trt_scaled<L>(gout, rho, delta, u, om, MASKED ? __ldg(&pe->omega_minus) : bulk.omega_minus);
           } else {
-            relax_bgk_scaled<L>(gout, rho, u, om);
+            relax_bgk_scaled<L>(gout, rho, delta, u, om);
           }
           r = rho;
           u2 = norm_sqr(u);

@@ -150,12 +150,14 @@ ensemble_step_kernel(float* __restrict__ pool, const InstanceDevice* __restrict_
         float rho, u[3];
         if (I.kind == OLB_B200_ENSEMBLE_CHANNEL) {
           const float gg[3] = {I.force[0], I.force[1], I.force[2]};
-          compute_rho_u_forced<L>(f, gg, rho, u);
-          relax_bgk<L>(f, rho, u, I.omega);
+          float delta;
+          compute_rho_delta_u_forced<L>(f, gg, rho, delta, u);
+          relax_bgk<L>(f, rho, delta, u, I.omega);
           add_force<L>(f, rho, u, I.force_relax, gg);
         } else {
-          compute_rho_u<L>(f, rho, u);
-          relax_bgk<L>(f, rho, u, I.omega);
+          float delta;
+          compute_rho_delta_u<L>(f, rho, delta, u);
+          relax_bgk<L>(f, rho, delta, u, I.omega);
         }
       } else {
         // moving lid: collision::NguyenLaddCorrection<Revert>

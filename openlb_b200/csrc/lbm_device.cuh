@@ -196,6 +196,34 @@ OLB_DEV void compute_rho_u_forced(const R (&f)[L::q], const R (&g)[3], R& rho, R
   u[0] += g[0] * R(0.5); u[1] += g[1] * R(0.5); u[2] += g[2] * R(0.5);
 }
 
+// The same moments plus the density deviation delta = rho - 1.  The shifted
+// populations sum to delta directly; rho = delta + 1 is then the value
+// lbm::computeRho gives.  The fast build's collisions use delta to form the
+// equilibrium without the rho*t - t cancellation, which at low Mach numbers
+// would cost FP32 most of the bits of the velocity term.
+template <class L, class R>
+OLB_DEV void compute_rho_delta_u(const R (&f)[L::q], R& rho, R& delta, R (&u)[3])
+{
+  R s = f[0];
+  static_for<1, L::q>([&](auto i) { s += f[i]; });
+  delta = s;
+  rho = s + R(1);
+  compute_j<L>(f, u);
+#ifdef OLB_B200_EXACT
+  u[0] /= rho; u[1] /= rho; u[2] /= rho;
+#else
+  const R inv = R(1) / rho;
+  u[0] *= inv; u[1] *= inv; u[2] *= inv;
+#endif
+}
+
+template <class L, class R>
+OLB_DEV void compute_rho_delta_u_forced(const R (&f)[L::q], const R (&g)[3], R& rho, R& delta, R (&u)[3])
+{
+  compute_rho_delta_u<L>(f, rho, delta, u);
+  u[0] += g[0] * R(0.5); u[1] += g[1] * R(0.5); u[2] += g[2] * R(0.5);
+}
+
 // util::normSqr  src/core/util.h:161-168
 template <class R>
 OLB_DEV R norm_sqr(const R (&u)[3])
@@ -271,27 +299,29 @@ OLB_DEV void relax_trt_reference(R (&f)[L::q], R rho, const R (&u)[3], R omega, 
 // The same two collisions evaluated over opposite pairs.  For c_o = -c_i the
 // second-order equilibria share their even part:
 //   feq_i = A + B,  feq_o = A - B,
-//   A = rho t (1 + 9/2 (c.u)^2 - 3/2 |u|^2) - t,   B = 3 rho t (c.u),
-// so each pair costs one c.u, one even and one odd term; products of rho with
-// a weight are shared between directions of the same weight.  Algebraically
-// identical to the reference; rounding differs by a few ulp.
+//   A = t (delta + rho (9/2 (c.u)^2 - 3/2 |u|^2)),   B = 3 rho t (c.u),
+// with delta = rho - 1 from the populations' sum (A = rho t X - t regrouped so
+// nothing cancels), so each pair costs one c.u, one even and one odd term.
+// Algebraically identical to the reference; rounding differs by a few ulp of
+// the populations, and at low Mach numbers FP32 keeps the velocity terms the
+// reference's form loses to the cancellation.
 template <class L, class R>
-OLB_DEV void relax_bgk_paired(R (&f)[L::q], R rho, const R (&u)[3], R omega)
+OLB_DEV void relax_bgk_paired(R (&f)[L::q], R rho, R delta, const R (&u)[3], R omega)
 {
   const R usqr = norm_sqr(u);
-  const R even0 = R(1) - R(1.5) * usqr;
+  const R e0 = R(-1.5) * usqr;
   const R keep = R(1) - omega;
   {
     constexpr R t = weight<L, R>(0);
-    f[0] = keep * f[0] + omega * (rho * t * even0 - t);
+    f[0] = keep * f[0] + omega * (t * (delta + rho * e0));
   }
   static_for<1, L::half + 1>([&](auto i) {
     constexpr int o = L::opp(i);
     constexpr R t = weight<L, R>(i);
-    const R rt = rho * t;
     const R cu = c_dot<L, i.value>(u);
-    const R a = rt * (even0 + R(4.5) * cu * cu) - t;
-    const R b = (rt * R(3)) * cu;
+    const R ev = R(4.5) * cu * cu + e0;
+    const R a = t * (delta + rho * ev);
+    const R b = (rho * (R(3) * t)) * cu;
     const R fi = keep * f[i] + omega * (a + b);
     const R fo = keep * f[o] + omega * (a - b);
     f[i] = fi;
@@ -300,21 +330,21 @@ OLB_DEV void relax_bgk_paired(R (&f)[L::q], R rho, const R (&u)[3], R omega)
 }
 
 template <class L, class R>
-OLB_DEV void relax_trt_paired(R (&f)[L::q], R rho, const R (&u)[3], R omega, R omega_minus)
+OLB_DEV void relax_trt_paired(R (&f)[L::q], R rho, R delta, const R (&u)[3], R omega, R omega_minus)
 {
   const R usqr = norm_sqr(u);
-  const R even0 = R(1) - R(1.5) * usqr;
+  const R e0 = R(-1.5) * usqr;
   {
     constexpr R t = weight<L, R>(0);
-    f[0] -= omega * (f[0] - (rho * t * even0 - t));
+    f[0] -= omega * (f[0] - t * (delta + rho * e0));
   }
   static_for<1, L::half + 1>([&](auto i) {
     constexpr int o = L::opp(i);
     constexpr R t = weight<L, R>(i);
-    const R rt = rho * t;
     const R cu = c_dot<L, i.value>(u);
-    const R a = rt * (even0 + R(4.5) * cu * cu) - t;  // symmetric part of feq
-    const R b = (rt * R(3)) * cu;                      // antisymmetric part
+    const R ev = R(4.5) * cu * cu + e0;
+    const R a = t * (delta + rho * ev);                 // symmetric part of feq
+    const R b = (rho * (R(3) * t)) * cu;                // antisymmetric part
     const R dp = omega * (R(0.5) * (f[i] + f[o]) - a);
     const R dm = omega_minus * (R(0.5) * (f[i] - f[o]) - b);
     const R fi = f[i] - dp - dm;
@@ -327,22 +357,24 @@ OLB_DEV void relax_trt_paired(R (&f)[L::q], R rho, const R (&u)[3], R omega, R o
 // The exact (-fmad=false) build keeps the reference's operation order so it
 // reproduces the reference bit for bit; the fast build uses the pair form.
 template <class L, class R>
-OLB_DEV void relax_bgk(R (&f)[L::q], R rho, const R (&u)[3], R omega)
+OLB_DEV void relax_bgk(R (&f)[L::q], R rho, R delta, const R (&u)[3], R omega)
 {
 #ifdef OLB_B200_EXACT
+  (void)delta;
   relax_bgk_reference<L>(f, rho, u, omega);
 #else
-  relax_bgk_paired<L>(f, rho, u, omega);
+  relax_bgk_paired<L>(f, rho, delta, u, omega);
 #endif
 }
 
 template <class L, class R>
-OLB_DEV void relax_trt(R (&f)[L::q], R rho, const R (&u)[3], R omega, R omega_minus)
+OLB_DEV void relax_trt(R (&f)[L::q], R rho, R delta, const R (&u)[3], R omega, R omega_minus)
 {
 #ifdef OLB_B200_EXACT
+  (void)delta;
   relax_trt_reference<L>(f, rho, u, omega, omega_minus);
 #else
-  relax_trt_paired<L>(f, rho, u, omega, omega_minus);
+  relax_trt_paired<L>(f, rho, delta, u, omega, omega_minus);
 #endif
 }
 
@@ -424,28 +456,28 @@ OLB_DEV void revert(R (&f)[L::q])
 template <class L, int KIND, class R>
 OLB_DEV void collide_bulk(R (&f)[L::q], const DynDevice<R>& p, R& st_rho, R& st_usqr)
 {
-  R rho, u[3];
+  R rho, delta, u[3];
   if constexpr (KIND == K_BGK) {
-    compute_rho_u<L>(f, rho, u);
-    relax_bgk<L>(f, rho, u, p.omega);
+    compute_rho_delta_u<L>(f, rho, delta, u);
+    relax_bgk<L>(f, rho, delta, u, p.omega);
     st_rho = rho; st_usqr = norm_sqr(u);
   } else if constexpr (KIND == K_TRT) {
-    compute_rho_u<L>(f, rho, u);
-    relax_trt<L>(f, rho, u, p.omega, p.omega_minus);
+    compute_rho_delta_u<L>(f, rho, delta, u);
+    relax_trt<L>(f, rho, delta, u, p.omega, p.omega_minus);
     st_rho = rho; st_usqr = norm_sqr(u);
   } else if constexpr (KIND == K_SMAGORINSKY) {
-    compute_rho_u<L>(f, rho, u);
+    compute_rho_delta_u<L>(f, rho, delta, u);
     const R w = smagorinsky_omega<L>(f, rho, u, p.smago_pre, p.tau_mol);
-    relax_bgk<L>(f, rho, u, w);
+    relax_bgk<L>(f, rho, delta, u, w);
     st_rho = rho; st_usqr = norm_sqr(u);
   } else if constexpr (KIND == K_FORCED_BGK || KIND == K_FORCED_TRT) {
     // forcing::Guo::combined_collision::apply  src/dynamics/forcing.h:53-63
     const R g[3] = {p.force[0], p.force[1], p.force[2]};
-    compute_rho_u_forced<L>(f, g, rho, u);
+    compute_rho_delta_u_forced<L>(f, g, rho, delta, u);
     if constexpr (KIND == K_FORCED_BGK) {
-      relax_bgk<L>(f, rho, u, p.omega);
+      relax_bgk<L>(f, rho, delta, u, p.omega);
     } else {
-      relax_trt<L>(f, rho, u, p.omega, p.omega_minus);
+      relax_trt<L>(f, rho, delta, u, p.omega, p.omega_minus);
     }
     add_force<L>(f, rho, u, p.force_relax, g);
     st_rho = rho; st_usqr = norm_sqr(u);
@@ -520,13 +552,14 @@ OLB_DEV void collide_interpolated(R (&f)[L::q], int kind, const DynDevice<R>* __
   const R* __restrict__ v = e->bc_values + 4 * size_t(bc_index(e, x, y, z));
   R rho, u[3];
   bc_rho_u<L>(f, kind, e->bc_dir, e->bc_orient, v, rho, u);
+  const R delta = rho - R(1);
   if constexpr (KIND == K_TRT) {
-    relax_trt<L>(f, rho, u, e->omega, e->omega_minus);
+    relax_trt<L>(f, rho, delta, u, e->omega, e->omega_minus);
   } else if constexpr (KIND == K_SMAGORINSKY) {
     const R w = smagorinsky_omega<L>(f, rho, u, e->smago_pre, e->tau_mol);
-    relax_bgk<L>(f, rho, u, w);
+    relax_bgk<L>(f, rho, delta, u, w);
   } else {
-    relax_bgk<L>(f, rho, u, e->omega);
+    relax_bgk<L>(f, rho, delta, u, e->omega);
   }
   st_rho = rho;
   st_usqr = norm_sqr(u);
@@ -564,7 +597,7 @@ OLB_HD constexpr float inv_class_scale(int k)
 }
 
 template <class L>
-OLB_DEV void scaled_rho_u(const float (&g)[L::q], float& rho, float (&u)[3])
+OLB_DEV void scaled_rho_u(const float (&g)[L::q], float& rho, float& delta, float (&u)[3])
 {
   float m[4] = {0.f, 0.f, 0.f, 0.f};
   float j[3][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
@@ -577,64 +610,66 @@ OLB_DEV void scaled_rho_u(const float (&g)[L::q], float& rho, float (&u)[3])
       else if constexpr (cc == -1) { j[d][k] -= g[i]; }
     });
   });
-  rho = 1.f;
+  delta = 0.f;
   u[0] = u[1] = u[2] = 0.f;
   static_for<0, 4>([&](auto k) {
     constexpr float inv = inv_class_scale<L>(k);
     if constexpr (inv != 0.f) {
-      rho += m[k] * inv;
+      delta += m[k] * inv;
       u[0] += j[0][k] * inv;
       u[1] += j[1][k] * inv;
       u[2] += j[2][k] * inv;
     }
   });
+  rho = delta + 1.f;
   const float r = 1.f / rho;
   u[0] *= r; u[1] *= r; u[2] *= r;
 }
 
 // BGK (pair form) on g, with omega folded into the equilibrium terms:
 // g_i' = (1 - omega) g_i + A + B, g_opp' = (1 - omega) g_opp + A - B,
-// A = omega s t (rho (1 + 9/2 (c.u)^2 - 3/2 |u|^2) - 1), B = 3 omega s t rho (c.u)
+// A = omega s t (delta + rho (9/2 (c.u)^2 - 3/2 |u|^2)), B = 3 omega s t rho (c.u)
 template <class L>
-OLB_DEV void relax_bgk_scaled(float (&g)[L::q], float rho, const float (&u)[3], float omega)
+OLB_DEV void relax_bgk_scaled(float (&g)[L::q], float rho, float delta, const float (&u)[3], float omega)
 {
   const float usqr = norm_sqr(u);
-  const float even0 = 1.f - 1.5f * usqr;
+  const float e0 = -1.5f * usqr;
   const float keep = 1.f - omega;
   {
     constexpr float T = storage_scale<L>(0) * weight<L, float>(0);
     const float wt = omega * T;
-    g[0] = keep * g[0] + ((rho * wt) * even0 - wt);
+    g[0] = keep * g[0] + wt * (delta + rho * e0);
   }
   static_for<1, L::half + 1>([&](auto i) {
     constexpr int o = L::opp(i);
     constexpr float T = storage_scale<L>(i) * weight<L, float>(i);
     const float wt = omega * T;
-    const float rwt = rho * wt;
     const float cu = c_dot<L, i.value>(u);
-    const float a = rwt * (even0 + 4.5f * cu * cu) - wt;
-    const float b = (rwt * 3.f) * cu;
+    const float ev = 4.5f * cu * cu + e0;
+    const float a = wt * (delta + rho * ev);
+    const float b = (rho * (3.f * wt)) * cu;
     g[i] = (keep * g[i] + a) + b;
     g[o] = (keep * g[o] + a) - b;
   });
 }
 
 template <class L>
-OLB_DEV void relax_trt_scaled(float (&g)[L::q], float rho, const float (&u)[3], float omega, float omega_minus)
+OLB_DEV void relax_trt_scaled(float (&g)[L::q], float rho, float delta, const float (&u)[3], float omega,
+                              float omega_minus)
 {
   const float usqr = norm_sqr(u);
-  const float even0 = 1.f - 1.5f * usqr;
+  const float e0 = -1.5f * usqr;
   {
     constexpr float T = storage_scale<L>(0) * weight<L, float>(0);
-    g[0] -= omega * (g[0] - (rho * T * even0 - T));
+    g[0] -= omega * (g[0] - T * (delta + rho * e0));
   }
   static_for<1, L::half + 1>([&](auto i) {
     constexpr int o = L::opp(i);
     constexpr float T = storage_scale<L>(i) * weight<L, float>(i);
-    const float rt = rho * T;
     const float cu = c_dot<L, i.value>(u);
-    const float a = rt * (even0 + 4.5f * cu * cu) - T;
-    const float b = (rt * 3.f) * cu;
+    const float ev = 4.5f * cu * cu + e0;
+    const float a = T * (delta + rho * ev);
+    const float b = (rho * (3.f * T)) * cu;
     const float dp = omega * (0.5f * (g[i] + g[o]) - a);
     const float dm = omega_minus * (0.5f * (g[i] - g[o]) - b);
     const float gi = g[i] - dp - dm;

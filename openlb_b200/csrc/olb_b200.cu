@@ -94,6 +94,46 @@ __global__ void velocity_residual_kernel(const R* __restrict__ u_now, R* __restr
   block_stats(du2, u2, 0., 0ull, 0ull, partials);
 }
 
+// splitmix64 (Steele, Lea, Flood, "Fast splittable pseudorandom number
+// generators", OOPSLA 2014): a counter-based uniform variate per key
+OLB_HD uint64_t splitmix64(uint64_t x)
+{
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Inlet fluctuations of step `step`: VELOCITY_d = base_d + amp |base| (2 r - 1)
+// on every interpolated velocity cell, r = splitmix64(seed + (step*cells +
+// cell)*3 + d) / 2^64 (53 bits).  Runs before the step's collision, so the
+// collision and the PostStream pass of that step see the same values.
+template <class R>
+__global__ void bc_noise_kernel(const uint32_t* __restrict__ cells, uint32_t count,
+                                const uint8_t* __restrict__ ids, const DynDevice<R>* __restrict__ table,
+                                const R* __restrict__ base_all, R* __restrict__ values_all, Geometry g,
+                                uint64_t step, uint64_t n_cells, double amp, uint64_t seed)
+{
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint32_t n = cells[k];
+  const DynDevice<R>* e = table + ids[n];
+  if (e->kind != K_INTERP_VELOCITY) return;
+  int x, y, z;
+  decode_cell(g, n, x, y, z);
+  const size_t slot = size_t(e->bc_values - static_cast<const R*>(values_all)) / 4 + bc_index(e, x, y, z);
+  const R* b = base_all + 4 * slot;
+  R* v = values_all + 4 * slot;
+  const double bu[3] = {double(b[1]), double(b[2]), double(b[3])};
+  const double mag = sqrt(bu[0] * bu[0] + bu[1] * bu[1] + bu[2] * bu[2]);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const uint64_t key = seed + (step * n_cells + n) * 3u + uint64_t(d);
+    const double r = double(splitmix64(key) >> 11) * 0x1.0p-53;
+    v[1 + d] = R(bu[d] + amp * mag * (2.0 * r - 1.0));
+  }
+}
+
 } // namespace olb_b200
 
 using namespace olb_b200;
@@ -239,6 +279,9 @@ struct olb_b200_lattice {
   void* bc_u = nullptr;             // device: 3 R per slot
   size_t bc_slots = 0;
   size_t bc_bytes = 0;
+  void* bc_base = nullptr;          // device: 4 R per slot, the values before fluctuations
+  double noise_amp = 0.0;           // inlet fluctuations (olb_b200_set_boundary_noise)
+  uint64_t noise_seed = 0;
   bool initialized = false;         // PostStream post-processors applied to the initial state
 };
 
@@ -343,9 +386,13 @@ olb_b200_status initialize_once(olb_b200_lattice* L)
   return OLB_B200_OK;
 }
 
+olb_b200_status boundary_noise(olb_b200_lattice* L);
+
 olb_b200_status enqueue_steps(olb_b200_lattice* L, int steps, bool stats_last)
 {
   for (int s = 0; s < steps; ++s) {
+    olb_b200_status nst = boundary_noise(L);
+    if (nst != OLB_B200_OK) return nst;
     const bool stats = stats_last && s == steps - 1;
     StepLaunch a;
     a.pops = L->pops;
@@ -384,6 +431,8 @@ olb_b200_status setup_boundaries(olb_b200_lattice* L, const uint8_t* ids, const 
   if (L->bc_cells) cudaFree(L->bc_cells);
   if (L->bc_values) cudaFree(L->bc_values);
   if (L->bc_u) cudaFree(L->bc_u);
+  if (L->bc_base) cudaFree(L->bc_base);
+  L->bc_base = nullptr;
   L->bc_cells = nullptr;
   L->bc_values = nullptr;
   L->bc_u = nullptr;
@@ -443,13 +492,41 @@ olb_b200_status setup_boundaries(olb_b200_lattice* L, const uint8_t* ids, const 
 olb_b200_status upload_boundary_values(olb_b200_lattice* L)
 {
   if (!L->bc_slots) return OLB_B200_OK;
+  if (!L->bc_base) {
+    OLB_CUDA(cudaMalloc(&L->bc_base, 4 * L->bc_slots * L->real));
+    L->bc_bytes += 4 * L->bc_slots * L->real;
+    L->device_bytes += 4 * L->bc_slots * L->real;
+  }
   if (L->real == 8) {
     OLB_CUDA(cudaMemcpy(L->bc_values, L->bc_host.data(), L->bc_host.size() * sizeof(double),
+                        cudaMemcpyHostToDevice));
+    OLB_CUDA(cudaMemcpy(L->bc_base, L->bc_host.data(), L->bc_host.size() * sizeof(double),
                         cudaMemcpyHostToDevice));
   } else {
     std::vector<float> v(L->bc_host.begin(), L->bc_host.end());
     OLB_CUDA(cudaMemcpy(L->bc_values, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
+    OLB_CUDA(cudaMemcpy(L->bc_base, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
+  return OLB_B200_OK;
+}
+
+// inlet fluctuations of the step about to run (no-op unless enabled)
+olb_b200_status boundary_noise(olb_b200_lattice* L)
+{
+  if (L->noise_amp == 0.0 || L->n_bc == 0) return OLB_B200_OK;
+  const unsigned threads = 128, blocks = (L->n_bc + threads - 1) / threads;
+  if (L->real == 8) {
+    bc_noise_kernel<double><<<blocks, threads, 0, L->stream>>>(
+      L->bc_cells, L->n_bc, L->ids, static_cast<const DynDevice<double>*>(L->table),
+      static_cast<const double*>(L->bc_base), static_cast<double*>(L->bc_values), L->g, uint64_t(L->steps_done),
+      uint64_t(L->cells), L->noise_amp, L->noise_seed);
+  } else {
+    bc_noise_kernel<float><<<blocks, threads, 0, L->stream>>>(
+      L->bc_cells, L->n_bc, L->ids, static_cast<const DynDevice<float>*>(L->table),
+      static_cast<const float*>(L->bc_base), static_cast<float*>(L->bc_values), L->g, uint64_t(L->steps_done),
+      uint64_t(L->cells), L->noise_amp, L->noise_seed);
+  }
+  OLB_CUDA(cudaGetLastError());
   return OLB_B200_OK;
 }
 
@@ -568,6 +645,7 @@ void olb_b200_destroy(olb_b200_lattice* L)
   if (L->bc_cells) cudaFree(L->bc_cells);
   if (L->bc_values) cudaFree(L->bc_values);
   if (L->bc_u) cudaFree(L->bc_u);
+  if (L->bc_base) cudaFree(L->bc_base);
   if (L->stat_dev) cudaFree(L->stat_dev);
   if (L->stat_host) cudaFreeHost(L->stat_host);
   if (L->ev0) cudaEventDestroy(L->ev0);
@@ -933,6 +1011,21 @@ olb_b200_status olb_b200_set_boundary_values(olb_b200_lattice* L, const int64_t*
   }
   OLB_CUDA(cudaStreamSynchronize(L->stream));
   return upload_boundary_values(L);
+}
+
+olb_b200_status olb_b200_set_boundary_noise(olb_b200_lattice* L, double amplitude, uint64_t seed)
+{
+  g_last_error.clear();
+  if (!L) return fail(OLB_B200_ERR_ARG, "set_boundary_noise: null lattice");
+  if (!(amplitude >= 0.0 && amplitude < 1.0))
+    return fail(OLB_B200_ERR_ARG, "set_boundary_noise: amplitude %g outside [0,1)", amplitude);
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  L->noise_amp = amplitude;
+  L->noise_seed = seed;
+  if (amplitude == 0.0) return upload_boundary_values(L);  // back to the defined values
+  return OLB_B200_OK;
 }
 
 olb_b200_status olb_b200_initialize(olb_b200_lattice* L)

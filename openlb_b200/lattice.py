@@ -108,6 +108,28 @@ def InterpolatedPressureBoundary(mixin: Dynamics, direction: int, orientation: i
 
 FLUID_KINDS = {_abi.DYN_BGK, _abi.DYN_TRT, _abi.DYN_SMAGORINSKY, _abi.DYN_FORCED_BGK, _abi.DYN_FORCED_TRT}
 
+def splitmix64(x: np.ndarray) -> np.ndarray:
+    """splitmix64 (Steele, Lea, Flood, OOPSLA 2014) on uint64 arrays."""
+    x = np.asarray(x, dtype=np.uint64) + np.uint64(0x9E3779B97F4A7C15)
+    x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def inlet_noise(base_u: np.ndarray, cells: np.ndarray, step: int, n_cells: int, amplitude: float,
+                seed: int) -> np.ndarray:
+    """The inlet velocities olb_b200_set_boundary_noise gives cells ``cells``
+    (base velocities base_u, shape (k, 3)) before step ``step``."""
+    base_u = np.asarray(base_u, dtype=np.float64).reshape(-1, 3)
+    cells = np.asarray(cells, dtype=np.uint64).reshape(-1, 1)
+    d = np.arange(3, dtype=np.uint64).reshape(1, 3)
+    with np.errstate(over="ignore"):
+        key = np.uint64(seed) + (np.uint64(step) * np.uint64(n_cells) + cells) * np.uint64(3) + d
+        r = (splitmix64(key) >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+    mag = np.sqrt(np.sum(base_u * base_u, axis=1, keepdims=True))
+    return base_u + amplitude * mag * (2.0 * r - 1.0)
+
+
 # ---------------------------------------------------------------------------
 # block-level handle
 
@@ -183,6 +205,12 @@ class Lattice:
             raise ValueError(f"{cells.size} cells need {4 * cells.size} values, got {values.size}")
         self._check(self._lib.olb_b200_set_boundary_values(self._h, cells.ctypes.data, cells.size,
                                                            values.ctypes.data))
+
+    def set_boundary_noise(self, amplitude: float, seed: int = 0) -> None:
+        """Per-step inlet fluctuations of relative size ``amplitude`` (see
+        olb_b200_set_boundary_noise; :func:`inlet_noise` computes the same
+        values on the host)."""
+        self._check(self._lib.olb_b200_set_boundary_noise(self._h, float(amplitude), int(seed) & (2 ** 64 - 1)))
 
     def initialize(self) -> None:
         """SuperLattice::initialize: the PostStream post-processors once on the

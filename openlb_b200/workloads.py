@@ -8,6 +8,10 @@
 * :func:`cavity` — lid-driven cavity geometry as cavity3dBenchmark builds it
   (examples/laminar/cavity3dBenchmark/cavity3d.cpp:40-59): bounce-back walls on
   the box surface, a moving lid on the y = max face.
+* :func:`porous_spheres` — x-periodic channel with bounce-back walls at the y/z
+  faces and seeded non-overlapping spheres up to a solid fraction.
+* :func:`square_cylinder_channel` — channel with bounce-back y/z walls, an inlet
+  plane at x = 0, an outlet plane at x = nx-1 and a square cylinder spanning z.
 """
 from __future__ import annotations
 
@@ -73,4 +77,62 @@ def cavity(size):
     return ids.reshape(-1)
 
 
-__all__ = ["taylor_green", "tgv_velocity", "tgv_energy", "tgv_energy_decay", "cavity", "D3Q19"]
+def porous_spheres(size, r_range=(6.0, 14.0), solid_fraction=0.35, seed: int = 0, max_tries: int = 400000):
+    """Per-cell ids (0 fluid, 1 solid) of an x-periodic channel: bounce-back
+    walls on the y/z faces and spheres of radius uniform in r_range, centres
+    uniform in the box (periodic in x), overlaps rejected, added until the
+    solid fraction reaches ``solid_fraction`` (or ``max_tries`` candidates).
+    Returns (ids, number of spheres, solid fraction)."""
+    nx, ny, nz = size
+    solid = np.zeros(size, bool)
+    solid[:, 0, :] = solid[:, -1, :] = True
+    solid[:, :, 0] = solid[:, :, -1] = True
+    rng = np.random.default_rng(seed)
+    centres = np.zeros((0, 3))
+    radii = np.zeros(0)
+    count = int(solid.sum())
+    target = solid_fraction * solid.size
+    tries = 0
+    while count < target and tries < max_tries:
+        tries += 1
+        r = rng.uniform(*r_range)
+        c = rng.uniform([0.0, 1.0 + r, 1.0 + r], [nx, ny - 1.0 - r, nz - 1.0 - r])
+        if len(radii):
+            d = np.abs(centres - c)
+            d[:, 0] = np.minimum(d[:, 0], nx - d[:, 0])
+            if np.any(np.sum(d * d, axis=1) < (radii + r) ** 2):
+                continue
+        centres = np.vstack([centres, c])
+        radii = np.append(radii, r)
+        lo = np.floor(c - r).astype(int)
+        hi = np.ceil(c + r).astype(int) + 1
+        xs = np.arange(lo[0], hi[0])
+        ys = np.arange(max(lo[1], 0), min(hi[1], ny))
+        zs = np.arange(max(lo[2], 0), min(hi[2], nz))
+        X, Y, Z = np.meshgrid(xs, ys, zs, indexing="ij")
+        inside = (X + 0.5 - c[0]) ** 2 + (Y + 0.5 - c[1]) ** 2 + (Z + 0.5 - c[2]) ** 2 <= r * r
+        xi = np.mod(X[inside], nx)
+        block = solid[xi, Y[inside], Z[inside]]
+        count += int((~block).sum())
+        solid[xi, Y[inside], Z[inside]] = True
+    return solid.astype(np.uint8).reshape(-1), len(radii), count / solid.size
+
+
+def square_cylinder_channel(size, side: int = 32, x_centre: float | None = None):
+    """Per-cell ids of a channel: 0 fluid, 1 bounce-back (y/z walls and a
+    side x side square cylinder spanning z between the walls), 2 inlet plane
+    (x = 0, interior y/z), 3 outlet plane (x = nx-1, interior y/z)."""
+    nx, ny, nz = size
+    ids = np.zeros(size, np.uint8)
+    ids[:, 0, :] = ids[:, -1, :] = 1
+    ids[:, :, 0] = ids[:, :, -1] = 1
+    ids[0, 1:-1, 1:-1] = 2
+    ids[-1, 1:-1, 1:-1] = 3
+    xc = nx / 4 if x_centre is None else x_centre
+    x0, y0 = int(round(xc - side / 2)), ny // 2 - side // 2
+    ids[x0:x0 + side, y0:y0 + side, 1:-1] = 1
+    return ids.reshape(-1)
+
+
+__all__ = ["taylor_green", "tgv_velocity", "tgv_energy", "tgv_energy_decay", "cavity", "porous_spheres",
+           "square_cylinder_channel", "D3Q19"]

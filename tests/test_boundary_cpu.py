@@ -86,3 +86,24 @@ def test_interpolated_entries_from_dynamics():
     assert p.omega == 1.7 and p.smagorinsky == 0.13
     assert O.INTERP_VELOCITY == _abi.DYN_INTERPOLATED_VELOCITY
     assert O.INTERP_PRESSURE == _abi.DYN_INTERPOLATED_PRESSURE
+
+
+def test_inlet_noise_is_splitmix64():
+    from openlb_b200.lattice import inlet_noise
+
+    def sm64(x):
+        m = 2 ** 64
+        x = (x + 0x9E3779B97F4A7C15) % m
+        x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) % m
+        x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) % m
+        return x ^ (x >> 31)
+
+    base = np.array([[0.05, 0.001, -0.002], [0.04, 0.0, 0.0]])
+    cells = np.array([17, 123456789])
+    got = inlet_noise(base, cells, step=7, n_cells=10 ** 9, amplitude=0.02, seed=2 ** 63 + 5)
+    for j in range(2):
+        mag = float(np.linalg.norm(base[j]))
+        for d in range(3):
+            key = (2 ** 63 + 5 + (7 * 10 ** 9 + int(cells[j])) * 3 + d) % 2 ** 64
+            r = (sm64(key) >> 11) * 2.0 ** -53
+            assert got[j, d] == base[j, d] + 0.02 * mag * (2 * r - 1)

@@ -194,3 +194,41 @@ def test_superlattice_facade_channel():
     _, r_u = O.moments(case, np.nan_to_num(ref))
     fluid = case.dyn_id == 0
     np.testing.assert_allclose(got_u[:, fluid], r_u[:, fluid], rtol=0, atol=1e-6)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f64"])
+def test_inlet_fluctuations_match_host_emulation(storage):
+    """Per-step inlet fluctuations on the device equal defineU with the same
+    counter-based values before every step (emulated on the oracle)."""
+    from openlb_b200.lattice import inlet_noise
+    dtype = np.float64 if storage == "f64" else np.float32
+    case = C.interpolated_channel_case(19, (16, 10, 9), seed=6)
+    f0 = C.rest_state(19, case.n, dtype)
+    amp, seed, steps = 0.02, 12345, 12
+    lat = ob.Lattice(19, case.size, case.periodic, storage=storage)
+    try:
+        lat.set_dynamics(C.to_abi_table(case), case.dyn_id)
+        cells, values = C.boundary_cells_and_values(case)
+        lat.set_boundary_values(cells, values)
+        lat.set_boundary_noise(amp, seed)
+        lat.set_populations(f0)
+        lat.collide_and_stream(steps)
+        got = lat.get_populations()
+    finally:
+        lat.close()
+    inlet = cells[np.array([case.table[i].kind for i in case.dyn_id[cells]]) == O.INTERP_VELOCITY]
+    base = case.bc_values.copy()
+    f = f0.copy()
+    O.post_process(case, f)
+    for t in range(steps):
+        vals = base.copy()
+        vals[1:, inlet] = inlet_noise(base[1:, inlet].T, inlet, t, case.n, amp, seed).T
+        step_case = O.Case(q=case.q, size=case.size, periodic=case.periodic, table=case.table,
+                           dyn_id=case.dyn_id, bc_values=vals)
+        O.step(step_case, f, 1)
+    tol = 1e-12 if storage == "f64" else 1e-5
+    rel, _ = C.pop_tolerance_violation(19, got, f, tol)
+    assert rel <= tol, rel
+    # and the fluctuations did something
+    plain = run_oracle(case, f0, steps)
+    assert np.nanmax(np.abs(plain - f)) > 1e-6
