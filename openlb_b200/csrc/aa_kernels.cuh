@@ -522,21 +522,23 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
       float r = 0.f, u2 = 0.f;
       bool counted = false, done = false;
 #ifndef OLB_B200_EXACT
-      if constexpr (KIND == K_BGK || KIND == K_TRT) {
-        if (!MASKED || kind == KIND) {
-          float rho, delta, u[3];
-          scaled_rho_u<L>(gout, rho, delta, u);
-          const float om = MASKED ? __ldg(&pe->omega) : bulk.omega;
-          if constexpr (KIND == K_TRT) {
-            relax_trt_scaled<L>(gout, rho, delta, u, om, MASKED ? __ldg(&pe->omega_minus) : bulk.omega_minus);
-          } else {
-            relax_bgk_scaled<L>(gout, rho, delta, u, om);
-          }
-          r = rho;
-          u2 = norm_sqr(u);
-          counted = true;
-          done = true;
+      if (!MASKED || kind == KIND) {
+        if constexpr (MASKED) {
+          DynDevice<float> q;
+          q.omega = __ldg(&pe->omega);
+          q.omega_minus = __ldg(&pe->omega_minus);
+          q.smago_pre = __ldg(&pe->smago_pre);
+          q.tau_mol = __ldg(&pe->tau_mol);
+          q.force[0] = __ldg(&pe->force[0]);
+          q.force[1] = __ldg(&pe->force[1]);
+          q.force[2] = __ldg(&pe->force[2]);
+          q.force_relax = __ldg(&pe->force_relax);
+          collide_scaled<L, KIND>(gout, q, r, u2);
+        } else {
+          collide_scaled<L, KIND>(gout, bulk, r, u2);
         }
+        counted = true;
+        done = true;
       }
 #endif
       if (!done) {

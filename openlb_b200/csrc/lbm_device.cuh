@@ -428,12 +428,47 @@ OLB_DEV R pi_neq_norm_sqr(const R (&f)[L::q], R rho, const R (&u)[3])
   return n2;
 }
 
-// detail::SmagorinskyEffectiveOmega::computeEffectiveOmega
-// src/dynamics/collisionLES.h:59-80
+// The same norm for the fast build: c_a c_b is even in c, so a population and
+// its opposite enter every component of Pi as their sum (half the additions);
+// the (rho - 1) term uses the populations' sum delta; the norm is formed in R.
+// Algebraically the reference's quantity.
 template <class L, class R>
-OLB_DEV R smagorinsky_omega(const R (&f)[L::q], R rho, const R (&u)[3], R smago_pre, R tau_mol)
+OLB_DEV R pi_neq_norm_sqr_pairs(const R (&f)[L::q], R rho, R delta, const R (&u)[3])
 {
+  R P[L::half + 1];
+  static_for<1, L::half + 1>([&](auto i) { P[i] = f[i] + f[L::opp(i)]; });
+  R pi[6];
+  static_for<0, 3>([&](auto a) {
+    static_for<a.value, 3>([&](auto b) {
+      constexpr int k = a.value * 3 - (a.value * (a.value - 1)) / 2 + (b.value - a.value);
+      R s = R(0);
+      static_for<1, L::half + 1>([&](auto i) {
+        constexpr int cc = L::c(i, a) * L::c(i, b);
+        if constexpr (cc == 1) { s += P[i]; }
+        else if constexpr (cc == -1) { s -= P[i]; }
+      });
+      s -= rho * u[a] * u[b];
+      if constexpr (a.value == b.value) {
+        s -= R(1) / R(3) * delta;
+      }
+      pi[k] = s;
+    });
+  });
+  return pi[0] * pi[0] + pi[3] * pi[3] + pi[5] * pi[5] + R(2) * (pi[1] * pi[1] + pi[2] * pi[2] + pi[4] * pi[4]);
+}
+
+// detail::SmagorinskyEffectiveOmega::computeEffectiveOmega
+// src/dynamics/collisionLES.h:59-80 (the exact build keeps the reference's
+// norm; the fast build uses the pair-summed one)
+template <class L, class R>
+OLB_DEV R smagorinsky_omega(const R (&f)[L::q], R rho, R delta, const R (&u)[3], R smago_pre, R tau_mol)
+{
+#ifdef OLB_B200_EXACT
+  (void)delta;
   const R pnorm = sqrt(pi_neq_norm_sqr<L>(f, rho, u));
+#else
+  const R pnorm = sqrt(pi_neq_norm_sqr_pairs<L>(f, rho, delta, u));
+#endif
   const R tau_turb = R(0.5) * (sqrt(tau_mol * tau_mol + smago_pre / rho * pnorm) - tau_mol);
   const R tau_eff = tau_mol + tau_turb;
   return R(1) / tau_eff;
@@ -467,7 +502,7 @@ OLB_DEV void collide_bulk(R (&f)[L::q], const DynDevice<R>& p, R& st_rho, R& st_
     st_rho = rho; st_usqr = norm_sqr(u);
   } else if constexpr (KIND == K_SMAGORINSKY) {
     compute_rho_delta_u<L>(f, rho, delta, u);
-    const R w = smagorinsky_omega<L>(f, rho, u, p.smago_pre, p.tau_mol);
+    const R w = smagorinsky_omega<L>(f, rho, delta, u, p.smago_pre, p.tau_mol);
     relax_bgk<L>(f, rho, delta, u, w);
     st_rho = rho; st_usqr = norm_sqr(u);
   } else if constexpr (KIND == K_FORCED_BGK || KIND == K_FORCED_TRT) {
@@ -556,7 +591,7 @@ OLB_DEV void collide_interpolated(R (&f)[L::q], int kind, const DynDevice<R>* __
   if constexpr (KIND == K_TRT) {
     relax_trt<L>(f, rho, delta, u, e->omega, e->omega_minus);
   } else if constexpr (KIND == K_SMAGORINSKY) {
-    const R w = smagorinsky_omega<L>(f, rho, u, e->smago_pre, e->tau_mol);
+    const R w = smagorinsky_omega<L>(f, rho, delta, u, e->smago_pre, e->tau_mol);
     relax_bgk<L>(f, rho, delta, u, w);
   } else {
     relax_bgk<L>(f, rho, delta, u, e->omega);
@@ -677,6 +712,89 @@ OLB_DEV void relax_trt_scaled(float (&g)[L::q], float rho, float delta, const fl
     g[i] = gi;
     g[o] = go;
   });
+}
+
+// Smagorinsky effective omega from the scaled populations: Pi_ab per weight
+// class from pair sums (g_i + g_opp), one multiply by 1/s per class.
+template <class L>
+OLB_DEV float smagorinsky_omega_scaled(const float (&g)[L::q], float rho, float delta, const float (&u)[3],
+                                       float smago_pre, float tau_mol)
+{
+  float pik[6][4] = {};
+  static_for<1, L::half + 1>([&](auto i) {
+    constexpr int k = weight_class<L>(i);
+    const float P = g[i] + g[L::opp(i)];
+    static_for<0, 3>([&](auto a) {
+      static_for<a.value, 3>([&](auto b) {
+        constexpr int m = a.value * 3 - (a.value * (a.value - 1)) / 2 + (b.value - a.value);
+        constexpr int cc = L::c(i, a) * L::c(i, b);
+        if constexpr (cc == 1) { pik[m][k] += P; }
+        else if constexpr (cc == -1) { pik[m][k] -= P; }
+      });
+    });
+  });
+  float pi[6];
+  static_for<0, 3>([&](auto a) {
+    static_for<a.value, 3>([&](auto b) {
+      constexpr int m = a.value * 3 - (a.value * (a.value - 1)) / 2 + (b.value - a.value);
+      float s = 0.f;
+      static_for<1, 4>([&](auto k) {
+        constexpr float inv = inv_class_scale<L>(k);
+        if constexpr (inv != 0.f) { s += pik[m][k] * inv; }
+      });
+      s -= rho * u[a] * u[b];
+      if constexpr (a.value == b.value) { s -= (1.f / 3.f) * delta; }
+      pi[m] = s;
+    });
+  });
+  const float n2 = pi[0] * pi[0] + pi[3] * pi[3] + pi[5] * pi[5] + 2.f * (pi[1] * pi[1] + pi[2] * pi[2] + pi[4] * pi[4]);
+  const float tau_turb = 0.5f * (sqrtf(tau_mol * tau_mol + smago_pre / rho * sqrtf(n2)) - tau_mol);
+  return 1.f / (tau_mol + tau_turb);
+}
+
+// Guo forcing (lbm::addExternalForce, src/dynamics/lbm.h:544-566) on g: the
+// term of population i scaled by s_i (folded into s_i t_i)
+template <class L>
+OLB_DEV void add_force_scaled(float (&g)[L::q], float rho, const float (&u)[3], float force_relax,
+                              const float (&gf)[3])
+{
+  static_for<0, L::q>([&](auto i) {
+    constexpr float T = storage_scale<L>(i) * weight<L, float>(i);
+    const float cu = 9.f * c_dot<L, i.value>(u);
+    float term = 0.f;
+    static_for<0, 3>([&](auto d) {
+      constexpr int cc = L::c(i, d);
+      term += ((float(cc) - u[d]) * 3.f + cu * float(cc)) * gf[d];
+    });
+    g[i] += term * (T * force_relax * rho);
+  });
+}
+
+// Any fluid collision on the scaled 16-bit representation (see above).
+template <class L, int KIND>
+OLB_DEV void collide_scaled(float (&g)[L::q], const DynDevice<float>& p, float& st_rho, float& st_usqr)
+{
+  float rho, delta, u[3];
+  scaled_rho_u<L>(g, rho, delta, u);
+  constexpr bool forced = KIND == K_FORCED_BGK || KIND == K_FORCED_TRT;
+  float gf[3] = {0.f, 0.f, 0.f};
+  if constexpr (forced) {
+    gf[0] = p.force[0]; gf[1] = p.force[1]; gf[2] = p.force[2];
+    u[0] += gf[0] * 0.5f; u[1] += gf[1] * 0.5f; u[2] += gf[2] * 0.5f;
+  }
+  if constexpr (KIND == K_TRT || KIND == K_FORCED_TRT) {
+    relax_trt_scaled<L>(g, rho, delta, u, p.omega, p.omega_minus);
+  } else if constexpr (KIND == K_SMAGORINSKY) {
+    const float w = smagorinsky_omega_scaled<L>(g, rho, delta, u, p.smago_pre, p.tau_mol);
+    relax_bgk_scaled<L>(g, rho, delta, u, w);
+  } else {
+    relax_bgk_scaled<L>(g, rho, delta, u, p.omega);
+  }
+  if constexpr (forced) {
+    add_force_scaled<L>(g, rho, u, p.force_relax, gf);
+  }
+  st_rho = rho;
+  st_usqr = norm_sqr(u);
 }
 
 // collision::NguyenLaddCorrection<Revert>  src/dynamics/collision.h:333-346

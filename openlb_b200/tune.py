@@ -3,7 +3,8 @@
     python -m openlb_b200.tune [--n 256] [--steps 20] [--repeat 3]
 
 For each lattice class (D3Q19 FP32 periodic, D3Q19 FP32 cavity with walls and
-a lid, D3Q19 FP16/BF16, D3Q19 FP64, D3Q27 FP32/FP16) it times every
+a lid, D3Q19 FP16/BF16, D3Q19 FP64, D3Q27 FP32/FP16, forced TRT and
+Smagorinsky-BGK in FP32 and 16-bit storage) it times every
 step-kernel variant at every launch shape with CUDA events (best of
 `--repeat` runs of `--steps` steps), then runs the autotuner and prints one
 JSON line per measurement and a markdown summary of the fraction of the
@@ -18,19 +19,32 @@ from pathlib import Path
 import numpy as np
 
 from . import _abi
-from .lattice import BGKdynamics, BounceBack, BounceBackVelocity, Lattice
+from .lattice import (BGKdynamics, BounceBack, BounceBackVelocity, ForcedTRTdynamics, Lattice,
+                      SmagorinskyBGKdynamics)
 from .workloads import cavity
 
 BYTES = {"f32": 4, "f64": 8, "f16": 2, "bf16": 2}
 CLASSES = [
-    ("D3Q19 f32", 19, "f32", False),
-    ("D3Q19 f32 cavity", 19, "f32", True),
-    ("D3Q19 f16", 19, "f16", False),
-    ("D3Q19 bf16", 19, "bf16", False),
-    ("D3Q19 f64", 19, "f64", False),
-    ("D3Q27 f32", 27, "f32", False),
-    ("D3Q27 f16", 27, "f16", False),
+    ("D3Q19 f32", 19, "f32", False, "bgk"),
+    ("D3Q19 f32 cavity", 19, "f32", True, "bgk"),
+    ("D3Q19 f16", 19, "f16", False, "bgk"),
+    ("D3Q19 bf16", 19, "bf16", False, "bgk"),
+    ("D3Q19 f64", 19, "f64", False, "bgk"),
+    ("D3Q27 f32", 27, "f32", False, "bgk"),
+    ("D3Q27 f16", 27, "f16", False, "bgk"),
+    ("D3Q19 f32 forced TRT", 19, "f32", False, "forced_trt"),
+    ("D3Q19 f16 forced TRT", 19, "f16", False, "forced_trt"),
+    ("D3Q27 f32 Smagorinsky", 27, "f32", False, "smagorinsky"),
+    ("D3Q27 bf16 Smagorinsky", 27, "bf16", False, "smagorinsky"),
 ]
+
+
+def fluid(collision: str):
+    if collision == "smagorinsky":
+        return SmagorinskyBGKdynamics(omega=1.9, smagorinsky=0.1)
+    if collision == "forced_trt":
+        return ForcedTRTdynamics(omega=1.25, magic=3 / 16, force=(1e-6, 0.0, 0.0))
+    return BGKdynamics(omega=1.6)
 
 
 def peak_gbs() -> float:
@@ -41,13 +55,13 @@ def peak_gbs() -> float:
         return 6650.0
 
 
-def make_lattice(q, n, storage, masked):
+def make_lattice(q, n, storage, masked, collision="bgk"):
     lat = Lattice(q, (n, n, n), (not masked,) * 3, storage=storage)
     if masked:
-        lat.set_dynamics([BGKdynamics(omega=1.6), BounceBack(), BounceBackVelocity((0.1, 0.0, 0.0))],
+        lat.set_dynamics([fluid(collision), BounceBack(), BounceBackVelocity((0.1, 0.0, 0.0))],
                          cavity((n, n, n)))
     else:
-        lat.set_dynamics([BGKdynamics(omega=1.6)])
+        lat.set_dynamics([fluid(collision)])
     return lat
 
 
@@ -90,13 +104,16 @@ def main(argv=None):
     ap.add_argument("--variant", type=int, default=-1)
     ap.add_argument("--shape", default="128,2")
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--classes", default="", help="';'-separated substrings of the class labels to run")
     args = ap.parse_args(argv)
     if args.single:
         return run_single(args)
     peak = peak_gbs()
     summary = {}
-    for label, q, storage, masked in CLASSES:
-        lat = make_lattice(q, args.n, storage, masked)
+    for label, q, storage, masked, collision in CLASSES:
+        if args.classes and not any(c in label for c in args.classes.split(";")):
+            continue
+        lat = make_lattice(q, args.n, storage, masked, collision)
         cells = args.n ** 3
         bpc = 2 * q * BYTES[storage]
         best_fixed = {}
