@@ -60,7 +60,8 @@ def test_config3_runner_small():
 
 
 def test_config4_runner_small():
-    out = configs.c4(steps=300, size=(64, 32, 32), side=4, sample=50, storages=("f64", "bf16"))
+    out = configs.c4(steps=300, size=(64, 32, 32), side=4, sample=50, storages=("f64", "f64_other_seed", "bf16"))
     r = out["runs"]
     assert np.isfinite(r["bf16"]["time_avg_u_l2_vs_f64"]) and r["bf16"]["time_avg_u_l2_vs_f64"] < 0.05
+    assert 0 < r["f64_other_seed"]["time_avg_u_l2_vs_f64"] < 0.05
     assert 0.01 < r["f64"]["mean_ux_fluid"] < 0.1
