@@ -481,12 +481,14 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
     if (go[k]) {
       PairNeighbours nb(g, xp, y, z);
       static_for<0, Q>([&](auto i) {
+        // 32-bit element indices: the paired layout is only used while
+        // q * pstride < 2^32 (olb_b200_create)
         if constexpr (!ODD) {
-          raw[k][i] = pops[size_t(i.value) * pstride + e[k]];
+          raw[k][i] = pops[uint32_t(i.value) * pstride + e[k]];
         } else {
           constexpr int o = L::opp(i);
           const uint32_t src = nb.template at<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>();
-          const T v = pops[size_t(o) * pstride + src];
+          const T v = pops[uint32_t(o) * pstride + src];
           if constexpr (L::c(i, 0) != 0) {
             raw[k][i] = pair_perm(v, v, nb.swap[1 - L::c(i, 0)] ? 0x1032u : 0x3210u);
           } else {
@@ -582,14 +584,14 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
     static_for<0, Q>([&](auto i) {
       if constexpr (!ODD) {
         constexpr int o = L::opp(i);
-        pops[size_t(o) * ps + ek] = raw[k][i];
+        pops[uint32_t(o) * ps + ek] = raw[k][i];
       } else {
         const uint32_t dst = nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>();
         T v = raw[k][i];
         if constexpr (L::c(i, 0) != 0) {
           v = pair_perm(v, v, nb.swap[1 + L::c(i, 0)] ? 0x1032u : 0x3210u);
         }
-        pops[size_t(i.value) * ps + dst] = v;
+        pops[uint32_t(i.value) * ps + dst] = v;
       }
     });
   });

@@ -579,8 +579,10 @@ olb_b200_status olb_b200_create(const olb_b200_desc* desc, olb_b200_lattice** ou
   if (desc->nx > 65535) return fail(OLB_B200_ERR_ARG, "create: nx %d exceeds 65535", desc->nx);
   // 16-bit storage with an even nx uses the paired layout (two cells per
   // 4-byte element); its element columns start on 256-byte boundaries too
+  // (its kernel indexes elements with 32 bits: q * stride/2 < 2^32)
   const bool paired = (desc->storage == OLB_B200_STORAGE_F16 || desc->storage == OLB_B200_STORAGE_BF16) &&
-                      desc->nx % 2 == 0;
+                      desc->nx % 2 == 0 &&
+                      uint64_t(desc->q) * ((cells + 127) / 128 * 64) < (uint64_t(1) << 32);
   const size_t stride = paired ? (cells + 127) / 128 * 128 : (cells + 63) / 64 * 64;
   if (stride * size_t(desc->q) > (size_t(1) << 40)) return fail(OLB_B200_ERR_ARG, "create: lattice too large");
 
