@@ -123,6 +123,8 @@ ensemble_step_kernel(float* __restrict__ pool, const InstanceDevice* __restrict_
     const InstanceDevice& I = table[tile.inst];
     if (!I.active) continue;
     const bool odd = ((I.steps_done + uint32_t(k_in_chunk)) & 1u) != 0u;
+    // 32-bit element indices within the instance (ensemble_add keeps an
+    // instance's columns below 2^32 elements)
     float* __restrict__ pops = pool + I.pops;
     const uint32_t stride = I.stride;
     const Geometry g{I.nx, I.ny, I.nz, stride, 0};
@@ -139,11 +141,11 @@ ensemble_step_kernel(float* __restrict__ pool, const InstanceDevice* __restrict_
       Neighbours nb(g, int(x), int(y), int(z));
       float f[kQ];
       if (!odd) {
-        static_for<0, kQ>([&](auto i) { f[i] = pops[size_t(i.value) * stride + n]; });
+        static_for<0, kQ>([&](auto i) { f[i] = pops[uint32_t(i.value) * stride + n]; });
       } else {
         static_for<0, kQ>([&](auto i) {
           constexpr int o = L::opp(i);
-          f[i] = pops[size_t(o) * stride + nb.template at<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>()];
+          f[i] = pops[uint32_t(o) * stride + nb.template at<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>()];
         });
       }
       if (kind == CELL_FLUID) {
@@ -172,11 +174,11 @@ ensemble_step_kernel(float* __restrict__ pool, const InstanceDevice* __restrict_
       if (!odd) {
         static_for<0, kQ>([&](auto i) {
           constexpr int o = L::opp(i);
-          pops[size_t(o) * st + n] = f[i];
+          pops[uint32_t(o) * st + n] = f[i];
         });
       } else {
         static_for<0, kQ>([&](auto i) {
-          pops[size_t(i.value) * st + nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>()] = f[i];
+          pops[uint32_t(i.value) * st + nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>()] = f[i];
         });
       }
     }
@@ -597,7 +599,9 @@ olb_b200_status olb_b200_ensemble_add(olb_b200_ensemble* E, const olb_b200_insta
   if (d->nx < 3 || d->ny < 3 || d->nz < 3) return efail(OLB_B200_ERR_ARG, "ensemble_add: extent below 3");
   if (!(d->omega > 0.0 && d->omega < 2.0)) return efail(OLB_B200_ERR_ARG, "ensemble_add: omega outside (0,2)");
   const uint64_t cells = uint64_t(d->nx) * d->ny * d->nz;
-  if (cells >= (uint64_t(1) << 31)) return efail(OLB_B200_ERR_ARG, "ensemble_add: too many cells");
+  // the step kernel indexes an instance's populations with 32 bits
+  if (instance_elems(cells) >= (uint64_t(1) << 32))
+    return efail(OLB_B200_ERR_ARG, "ensemble_add: instance too large (q x cells must stay below 2^32)");
   int slot = -1;
   for (int s = 0; s < E->max_instances; ++s) {
     if (!E->used[s]) {
