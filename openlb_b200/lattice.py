@@ -527,6 +527,58 @@ class SuperLattice:
         if self._initialized:
             self.block.set_populations(self._pending_pops.reshape(-1))
 
+    # -- checkpoints in OpenLB's format (openlb_b200/checkpoint.py) ----------
+    def _checkpoint_fields(self, descriptor_fields):
+        """The fields OpenLB's block would serialize for this set-up
+        (checkpoint.setup_fields over this lattice's dynamics table)."""
+        from . import checkpoint as CK
+        if self._bc:
+            raise NotImplementedError("checkpoints of lattices with interpolated boundaries: their momenta "
+                                      "allocate one VELOCITY field per boundary normal")
+        table, ids = self._table()
+        return CK.setup_fields(self.descriptor.q, ids, table, descriptor_fields)
+
+    # Serializable::save(fileName) (core/serializer.hh:145-149), without the
+    # log-directory prefix: writes <fileName>_rank0_size1.dat
+    def save(self, fileName: str, descriptor_fields=("FORCE",), overlap: int = 3) -> str:
+        """Saves the lattice as OpenLB's ``SuperLattice::save`` does for a
+        one-block lattice whose descriptor carries ``descriptor_fields``
+        (``D3Q19<FORCE>`` by default) and whose geometry has ``overlap``
+        padding layers; returns the file's path."""
+        from . import checkpoint as CK
+        if not self._initialized:
+            self.initialize()
+        fields, values = self._checkpoint_fields(descriptor_fields)
+        values["POPULATION"] = self.block.get_populations().reshape(self.descriptor.q, -1)
+        path = CK.file_name(fileName)
+        CK.save(path, values, self.descriptor.q, self.geometry.size, self.geometry.periodic,
+                self.block.dtype, overlap, fields)
+        return path
+
+    # Serializable::load(fileName) (core/serializer.hh:151-156)
+    def load(self, fileName: str, descriptor_fields=("FORCE",)) -> bool:
+        """Resumes from ``<fileName>_rank0_size1.dat`` written by OpenLB or by
+        :meth:`save`; False when the file does not exist.  The set-up must be
+        the one that wrote the file: the file's other fields are checked
+        against it (ValueError if they differ)."""
+        from pathlib import Path
+
+        from . import checkpoint as CK
+        path = Path(CK.file_name(fileName))
+        if not path.exists():
+            return False
+        if not self._initialized:
+            self.initialize()
+        fields, expect = self._checkpoint_fields(descriptor_fields)
+        arrays, _ = CK.load(path, self.descriptor.q, self.geometry.size, self.block.dtype, fields)
+        for name, want in expect.items():
+            got = arrays[name]
+            if not np.array_equal(got, want.astype(got.dtype)):
+                raise ValueError(f"checkpoint field {name} differs from this lattice's set-up")
+        self._pending_pops[...] = arrays["POPULATION"]
+        self.block.set_populations(self._pending_pops.reshape(-1))
+        return True
+
     def close(self) -> None:
         self.block.close()
 

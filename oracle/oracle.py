@@ -240,8 +240,11 @@ def reference_binary(q: int, dtype, variant: str = "sisd") -> Path:
 
 def write_case(dirpath: Path, case: Case, steps: int, init: np.ndarray | None = None,
                rhou: np.ndarray | None = None, stats: bool = False, bench=None,
-               normals: bool = False):
-    """Write a case directory for olb_ref_driver (materials = dyn_id + 1)."""
+               normals: bool = False, load_checkpoint: bytes | None = None,
+               save_checkpoint: bool = False):
+    """Write a case directory for olb_ref_driver (materials = dyn_id + 1).
+    ``load_checkpoint``: file text OpenLB resumes from after initialize();
+    ``save_checkpoint``: OpenLB saves the lattice after the steps (ckpt_out)."""
     dirpath = Path(dirpath)
     dirpath.mkdir(parents=True, exist_ok=True)
     ids = case.dyn_id if case.dyn_id is not None else np.zeros(case.n, np.uint8)
@@ -287,6 +290,11 @@ def write_case(dirpath: Path, case: Case, steps: int, init: np.ndarray | None = 
         lines.append("stats 1")
     if bench is not None:
         lines.append(f"bench {bench[0]} {bench[1]}")
+    if load_checkpoint is not None:
+        (dirpath / "ckpt_in_rank0_size1.dat").write_bytes(load_checkpoint)
+        lines.append("load ckpt_in")
+    if save_checkpoint:
+        lines.append("save ckpt_out")
     (dirpath / "case.txt").write_text("\n".join(lines) + "\n")
 
 
@@ -319,13 +327,15 @@ def reference_normals(materials: np.ndarray, periodic, boundary_materials, q: in
 
 def run_reference(case: Case, steps: int, dtype, init: np.ndarray | None = None,
                   rhou: np.ndarray | None = None, variant: str = "sisd", stats: bool = False,
-                  threads: int | None = None, normals: bool = False):
-    """Run OpenLB itself; returns dict(pops, rho, u[, stats])."""
+                  threads: int | None = None, normals: bool = False,
+                  load_checkpoint: bytes | None = None, save_checkpoint: bool = False):
+    """Run OpenLB itself; returns dict(pops, rho, u[, stats][, checkpoint])."""
     binary = reference_binary(case.q, dtype, variant)
     if not binary.exists():
         raise RuntimeError(f"reference build missing: {binary} (make -C oracle/ref)")
     with tempfile.TemporaryDirectory() as d:
-        write_case(Path(d), case, steps, init=init, rhou=rhou, stats=stats, normals=normals)
+        write_case(Path(d), case, steps, init=init, rhou=rhou, stats=stats, normals=normals,
+                   load_checkpoint=load_checkpoint, save_checkpoint=save_checkpoint)
         env = dict(os.environ)
         if threads:
             env["OMP_NUM_THREADS"] = str(threads)
@@ -342,4 +352,6 @@ def run_reference(case: Case, steps: int, dtype, init: np.ndarray | None = None,
             out["stats"] = np.loadtxt(Path(d) / "out_stats.txt", ndmin=2)
         if normals:
             out["normals"] = np.fromfile(Path(d) / "out_normals.i32", dtype=np.int32).reshape(4, n)
+        if save_checkpoint:
+            out["checkpoint"] = (Path(d) / "ckpt_out_rank0_size1.dat").read_bytes()
         return out

@@ -37,6 +37,10 @@
  * with the fluid material 1 and the outside material 0; MIXIN is the bulk
  * dynamics named by `bcmixin`.  Their boundary values go through Cell::defineRho
  * and Cell::defineU (core/cell.h:194-198).
+ * Checkpoints: `save <name>` writes the lattice after the steps with
+ * SuperLattice::save (core/superLattice.hh:807-842) into <name>_rank0_size1.dat;
+ * `load <name>` resumes from such a file after initialize() instead of the
+ * initial state.
  * Bench mode (`bench <warmup> <steps>` in case.txt) prints one JSON line with
  * MLUPS measured by OpenLB's own util::Timer (utilities/timer.hh:36-76).
  */
@@ -82,6 +86,7 @@ struct Case {
   std::string bcMixin = "bgk";
   bool bcValues = false;
   int dumpNormals = 0;
+  std::string loadPath, savePath;             // checkpoints (Serializable), relative to the case dir
 };
 
 Case parse_case(const std::string& dir)
@@ -113,6 +118,8 @@ Case parse_case(const std::string& dir)
     else if (key == "bcmixin") { ls >> c.bcMixin; }
     else if (key == "bcvalues") { int b; ls >> b; c.bcValues = b; }
     else if (key == "normals") { ls >> c.dumpNormals; }
+    else if (key == "load") { ls >> c.loadPath; }
+    else if (key == "save") { ls >> c.savePath; }
     else if (key == "lattice" || key == "dtype") { /* informational, checked below */ }
     else { throw std::runtime_error("unknown key " + key); }
   }
@@ -326,6 +333,15 @@ int main(int argc, char* argv[])
 
   lattice.initialize();
 
+  // Resume from a checkpoint as the examples do (bifurcation3d.cpp:560):
+  // Serializable::load reads <name>_rank0_size1.dat (core/serializer.hh:64-79,
+  // io/fileName.hh:51-63) and postLoad() refreshes the cyclic columns.
+  if (!cs.loadPath.empty()) {
+    if (!lattice.template load<false>(dir + "/" + cs.loadPath)) {
+      throw std::runtime_error("cannot load checkpoint " + cs.loadPath);
+    }
+  }
+
   if (cs.benchWarmup >= 0) {
     for (int iT = 0; iT < cs.benchWarmup; ++iT) {
       lattice.collideAndStream();
@@ -364,6 +380,11 @@ int main(int argc, char* argv[])
       auto& st = lattice.getStatistics();
       statsOut << double(st.getAverageRho()) << " " << double(st.getAverageEnergy())
                << " " << double(st.getMaxU()) << "\n";
+    }
+  }
+  if (!cs.savePath.empty()) {
+    if (!lattice.template save<false>(dir + "/" + cs.savePath)) {
+      throw std::runtime_error("cannot save checkpoint " + cs.savePath);
     }
   }
   lattice.setProcessingContext(ProcessingContext::Evaluation);

@@ -9,7 +9,12 @@ Density3D / Velocity3D fields and per-step LatticeStatistics after the stated
 number of collideAndStream steps (after the lattice's initialize(), which
 applies the PostStream post-processors once to the initial state).
 
-    python tests/golden/make_golden.py        # needs oracle/_ref (make -C oracle/ref)
+    python tests/golden/make_golden.py [prefix]   # needs oracle/_ref (make -C oracle/ref)
+
+The checkpoint_* fixtures hold a file OpenLB saved (SuperLattice::save), the
+populations it dumped for the same state, this library's file for that state
+and OpenLB's run resumed from this library's file (SuperLattice::load), which
+the generator checks against OpenLB's uninterrupted run bit for bit.
 
 The C oracle is pinned against these fixtures in tests/test_oracle_golden.py.
 """
@@ -28,6 +33,7 @@ ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT))
 
 from oracle import oracle as O  # noqa: E402
+from openlb_b200 import checkpoint as CK  # noqa: E402
 from tests import cases as C  # noqa: E402
 
 
@@ -76,6 +82,68 @@ def fixture_cases():
     return out
 
 
+def checkpoint_cases():
+    """(name, case, initial state, steps before the save, steps after it, dtype,
+    descriptor fields, fields the set-up allocates) for the checkpoint fixtures."""
+    rng = np.random.default_rng(99)
+    out = []
+    case = C.periodic_case(19, (7, 6, 5), kind=O.BGK)
+    out.append(("checkpoint_periodic_q19_float32_bgk", case, C.random_state(19, case.n, np.float32, rng),
+                5, 4, np.float32, ("FORCE",), ()))
+    case = C.periodic_case(27, (6, 5, 4), kind=O.TRT)
+    out.append(("checkpoint_periodic_q27_float64_trt", case, C.random_state(27, case.n, np.float64, rng),
+                3, 3, np.float64, ("FORCE",), ()))
+    case = C.cavity_case(19, (9, 8, 7))
+    out.append(("checkpoint_cavity_q19_float64", case, C.rest_state(19, case.n, np.float64),
+                12, 8, np.float64, ("FORCE",), ("VELOCITY", "RHO")))
+    case = C.porous_case(19, (12, 9, 8), np.random.default_rng(7), g=1e-4)
+    out.append(("checkpoint_porous_q19_float32", case, C.rest_state(19, case.n, np.float32),
+                10, 6, np.float32, ("FORCE",), ("RHO",)))
+    return out
+
+
+def checkpoint_fixture(name, case, f0, steps, resume, dtype, dfields, efields):
+    """OpenLB saves after `steps`; this library's file for that state is written
+    and OpenLB resumes from it for `resume` steps, which must equal OpenLB's
+    own run of steps + resume."""
+    fields = CK.lattice_fields(case.q, dfields, efields)
+    saved = O.run_reference(case, steps, dtype, init=f0, threads=1, save_checkpoint=True)
+    arrays, overlap = CK.load_bytes(saved["checkpoint"], case.q, case.size, dtype, fields)
+    if not np.array_equal(arrays["POPULATION"].reshape(-1), saved["pops"]):
+        raise AssertionError(f"{name}: the file's populations differ from OpenLB's own dump")
+    ours = CK.encode_fields(arrays, case.q, case.size, case.periodic, dtype, overlap, fields)
+    resumed = O.run_reference(case, resume, dtype, init=f0, threads=1, load_checkpoint=ours)
+    straight = O.run_reference(case, steps + resume, dtype, init=f0, threads=1)
+    # slots fed from OpenLB's non-periodic padding (the outward slots of walls
+    # on the box faces) hold what OpenLB streamed out earlier, which only
+    # OpenLB's own file carries; the oracle marks them NaN and no fluid cell
+    # ever reads them
+    probe = np.ascontiguousarray(arrays["POPULATION"].reshape(-1)).copy()
+    O.step(case, probe, resume)
+    live = np.isfinite(probe)
+    if not np.array_equal(resumed["pops"][live], straight["pops"][live]):
+        raise AssertionError(f"{name}: OpenLB resumed from this library's file differs from its own run")
+    payload = {
+        "q": np.int32(case.q), "size": np.array(case.size, np.int32),
+        "periodic": np.array(case.periodic, np.int32), "overlap": np.int32(overlap),
+        "steps": np.int32(steps), "resume_steps": np.int32(resume),
+        "dyn_id": case.dyn_id if case.dyn_id is not None else np.zeros(case.n, np.uint8),
+        "table": np.array([[d.kind, d.omega, d.magic, d.smagorinsky, *d.force, *d.wall_u, d.wall_rho]
+                           for d in case.table], np.float64),
+        "descriptor_fields": np.array(dfields, dtype="U16"), "extra_fields": np.array(efields, dtype="U16"),
+        "init": f0, "pops_saved": saved["pops"], "pops_resumed": resumed["pops"],
+        "checkpoint_ref": np.frombuffer(saved["checkpoint"], np.uint8),
+        "checkpoint_ours": np.frombuffer(ours, np.uint8),
+        # the oracle restates the generic templates: bit-identical except the
+        # CSE-generated D3Q19 BGK, which agrees to rounding
+        "tolerance": np.float64(2e-6 if dtype == np.float32 else 1e-13),
+    }
+    for k, v in arrays.items():
+        if k != "POPULATION":
+            payload[f"field_{k}"] = v
+    return payload
+
+
 def normals_geometries():
     """Material layouts whose boundary cells (material 3) cover flat faces,
     edges and corners; fluid is material 1, walls 2, outside 0."""
@@ -113,9 +181,18 @@ def normals_geometries():
     return out
 
 
-def main():
-    manifest = {}
+def main(only: str | None = None):
+    """Regenerates every fixture, or only those whose name starts with `only`
+    (the manifest keeps the other entries)."""
+    mf = HERE / "MANIFEST.json"
+    manifest = json.loads(mf.read_text())["fixtures"] if (only and mf.exists()) else {}
+
+    def wanted(name):
+        return only is None or name.startswith(only)
+
     for name, mats, periodic in normals_geometries():
+        if not wanted(name):
+            continue
         ref = O.reference_normals(mats, periodic, boundary_materials=(3,))
         path = HERE / f"{name}.npz"
         np.savez_compressed(path, materials=mats, periodic=np.array(periodic, np.int32), normals=ref)
@@ -123,6 +200,8 @@ def main():
                           "sha256": hashlib.sha256(path.read_bytes()).hexdigest()}
         print(name, path.stat().st_size, "types", np.unique(ref[0][ref[0] >= 0], return_counts=True))
     for name, case, f0, steps, dtype, variant, stats in fixture_cases():
+        if not wanted(name):
+            continue
         # one thread: the reference applies post-processors in an OpenMP loop
         # in place, so neighbouring pressure-boundary cells race otherwise
         ref = O.run_reference(case, steps, dtype, init=f0, variant=variant, stats=stats, threads=1)
@@ -144,6 +223,15 @@ def main():
         manifest[name] = {"variant": variant, "dtype": np.dtype(dtype).name, "steps": steps,
                           "sha256": hashlib.sha256(path.read_bytes()).hexdigest()}
         print(name, path.stat().st_size)
+    for name, case, f0, steps, resume, dtype, dfields, efields in checkpoint_cases():
+        if not wanted(name):
+            continue
+        payload = checkpoint_fixture(name, case, f0, steps, resume, dtype, dfields, efields)
+        path = HERE / f"{name}.npz"
+        np.savez_compressed(path, **payload)
+        manifest[name] = {"variant": "sisd", "dtype": np.dtype(dtype).name, "steps": steps + resume,
+                          "sha256": hashlib.sha256(path.read_bytes()).hexdigest()}
+        print(name, path.stat().st_size)
     gxx = subprocess.run(["g++", "--version"], capture_output=True, text=True).stdout.splitlines()[0]
     (HERE / "MANIFEST.json").write_text(json.dumps(
         {"generator": "tests/golden/make_golden.py", "reference_build": "oracle/ref/Makefile",
@@ -153,4 +241,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else None)

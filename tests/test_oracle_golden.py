@@ -28,7 +28,7 @@ import pytest
 from oracle import oracle as O
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-FIXTURES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith("normals_"))
+FIXTURES = sorted(p.stem for p in GOLDEN.glob("*.npz") if not p.stem.startswith(("normals_", "checkpoint_")))
 
 
 def load(name):
