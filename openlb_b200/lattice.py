@@ -519,6 +519,22 @@ class SuperLattice:
         _, u = self.block.get_moments()
         return u.reshape((3,) + self.geometry.size)
 
+    # SuperLatticePhysPressure3D (functors/lattice/latticePhysPressure3D.hh): lattice
+    # pressure (rho - 1.0) / invCs2, a double expression rounded to T, then
+    # UnitConverter::getPhysPressure in T (core/unitConverter.h:417-420); only rho
+    # crosses PCIe
+    def getPhysPressure(self, conversionPressure: float, charPhysPressure: float = 0.0) -> np.ndarray:
+        rho = self.getDensity()
+        dt = rho.dtype.type
+        lattice_p = ((rho.astype(np.float64) - 1.0) / 3.0).astype(rho.dtype)
+        return dt(conversionPressure) * lattice_p + dt(charPhysPressure)
+
+    # SuperLatticePhysVelocity3D (functors/lattice/latticePhysVelocity3D.hh:74-85):
+    # UnitConverter::getPhysVelocity = conversionVelocity * u (core/unitConverter.h:293-296)
+    def getPhysVelocity(self, conversionVelocity: float) -> np.ndarray:
+        u = self.getVelocity()
+        return u.dtype.type(conversionVelocity) * u
+
     def getPopulations(self) -> np.ndarray:
         return self.block.get_populations().reshape(self.descriptor.q, -1)
 
