@@ -52,14 +52,33 @@ from . import _abi
 #   POPULATION, FORCE, VELOCITY  olb::descriptors (descriptor/fields.h:315-339);
 #                                VELOCITY is what defineU writes for moving walls
 #   RHO                          olb::momenta::FixedDensity::RHO
-#                                (dynamics/momenta/elements.h:238), allocated by
-#                                every bounce-back wall
+#                                (dynamics/momenta/elements.h:238): the density of
+#                                bounce-back walls and interpolated pressure cells
+#   BC_VELOCITY                  olb::momenta::FixedVelocityMomentumGeneric::VELOCITY
+#                                (elements.h:529): interpolated velocity cells
+#   PRESSURE_VELOCITY_<d><+|->   olb::momenta::FixedPressureMomentum<d,o>::VELOCITY:
+#                                interpolated pressure cells of outward normal (d, o)
 FIELD_KEYS = {
     "POPULATION": "N3olb5ArrayINS_11descriptors10POPULATIONEEE",
     "FORCE": "N3olb5ArrayINS_11descriptors5FORCEEEE",
     "VELOCITY": "N3olb5ArrayINS_11descriptors8VELOCITYEEE",
     "RHO": "N3olb5ArrayINS_7momenta12FixedDensity3RHOEEE",
+    "BC_VELOCITY": "N3olb5ArrayINS_7momenta28FixedVelocityMomentumGeneric8VELOCITYEEE",
 }
+_COMPONENTS = {"FORCE": 3, "VELOCITY": 3, "RHO": 1, "BC_VELOCITY": 3}
+
+
+def pressure_velocity_field(direction: int, orientation: int) -> str:
+    return f"PRESSURE_VELOCITY_{int(direction)}{'+' if orientation > 0 else '-'}"
+
+
+def field_key(name: str) -> str:
+    if name in FIELD_KEYS:
+        return FIELD_KEYS[name]
+    if name.startswith("PRESSURE_VELOCITY_") and len(name) == 20 and name[18] in "012" and name[19] in "+-":
+        o = "1" if name[19] == "+" else "n1"      # template argument -1 mangles as Lin1E
+        return f"N3olb5ArrayINS_7momenta21FixedPressureMomentumILi{name[18]}ELi{o}EE8VELOCITYEEE"
+    raise ValueError(f"unknown field {name!r}")
 
 
 @dataclass(frozen=True)
@@ -70,19 +89,19 @@ class FieldSpec:
 
     @property
     def key(self) -> str:
-        return FIELD_KEYS[self.name]
+        return field_key(self.name)
 
 
 def lattice_fields(q: int, descriptor_fields=(), extra_fields=()) -> list[FieldSpec]:
     """Serialized fields of a block in file order: POPULATION (q cyclic columns),
     the descriptor's own fields (e.g. ``("FORCE",)`` for ``D3Q19<FORCE>``) and
     the fields the set-up allocated, sorted by their type names."""
-    comps = {"POPULATION": q, "FORCE": 3, "VELOCITY": 3, "RHO": 1}
     names = {"POPULATION", *descriptor_fields, *extra_fields}
+    specs = []
     for n in names:
-        if n not in FIELD_KEYS:
-            raise ValueError(f"unknown field {n!r}")
-    specs = [FieldSpec(n, comps[n], cyclic=(n == "POPULATION")) for n in names]
+        field_key(n)
+        comps = q if n == "POPULATION" else _COMPONENTS.get(n, 3)
+        specs.append(FieldSpec(n, comps, cyclic=(n == "POPULATION")))
     return sorted(specs, key=lambda s: s.key)
 
 
@@ -91,39 +110,45 @@ _WALLS = (_abi.DYN_BOUNCE_BACK, _abi.DYN_BOUNCE_BACK_VELOCITY)
 _MOVING_WALL = _abi.DYN_BOUNCE_BACK_VELOCITY
 
 
-def setup_fields(q: int, ids: np.ndarray, table, descriptor_fields=("FORCE",)):
+def setup_fields(q: int, ids: np.ndarray, table, descriptor_fields=("FORCE",), bc_values=None):
     """The fields OpenLB's block serializes for a set-up given as a per-cell
     dynamics id and its table (entries with ``kind``, ``force``, ``wall_u``,
-    ``wall_rho``), with their values on the core cells: FORCE where
-    defineField<FORCE> set the force of a forced dynamics, descriptors::VELOCITY
-    where defineU set a moving wall, and the FixedDensity RHO that every
-    bounce-back wall allocates (its wall density).  Returns (field specs in
-    file order, {name: array[components, cells]})."""
+    ``wall_rho``, ``direction``, ``orientation``), with their values on the core
+    cells: FORCE where defineField<FORCE> set the force of a forced dynamics,
+    descriptors::VELOCITY where defineU set a moving wall, the FixedDensity RHO
+    of bounce-back walls (their wall density) and of interpolated pressure
+    cells, and the momenta VELOCITY fields of interpolated velocity and
+    pressure cells (``bc_values``: float[4][cells], the rho, u boundary values).
+    Returns (field specs in file order, {name: array[components, cells]})."""
     ids = np.asarray(ids).reshape(-1)
     n = ids.size
     kinds = [int(d.kind) for d in table]
-    values, extra = {}, []
+    if any(k in _abi.DYN_INTERPOLATED for k in kinds) and bc_values is None:
+        raise ValueError("interpolated boundaries need their boundary values")
+    values = {}
+
+    def field(name, comps):
+        if name not in values:
+            values[name] = np.zeros((comps, n))
+        return values[name]
+
     if "FORCE" in descriptor_fields:
-        f = np.zeros((3, n))
-        for k, d in enumerate(table):
-            if kinds[k] in _FORCED:
-                f[:, ids == k] = np.asarray(d.force, np.float64)[:, None]
-        values["FORCE"] = f
-    if _MOVING_WALL in kinds:
-        extra.append("VELOCITY")
-        u = np.zeros((3, n))
-        for k, d in enumerate(table):
-            if kinds[k] == _MOVING_WALL:
-                u[:, ids == k] = np.asarray(d.wall_u, np.float64)[:, None]
-        values["VELOCITY"] = u
-    if any(k in _WALLS for k in kinds):
-        extra.append("RHO")
-        r = np.zeros((1, n))
-        for k, d in enumerate(table):
-            if kinds[k] in _WALLS:
-                r[0, ids == k] = d.wall_rho
-        values["RHO"] = r
-    return lattice_fields(q, tuple(descriptor_fields), tuple(extra)), values
+        field("FORCE", 3)
+    for k, d in enumerate(table):
+        sel = ids == k
+        if kinds[k] in _FORCED and "FORCE" in descriptor_fields:
+            values["FORCE"][:, sel] = np.asarray(d.force, np.float64)[:, None]
+        if kinds[k] == _MOVING_WALL:
+            field("VELOCITY", 3)[:, sel] = np.asarray(d.wall_u, np.float64)[:, None]
+        if kinds[k] in _WALLS:
+            field("RHO", 1)[0, sel] = d.wall_rho
+        if kinds[k] == _abi.DYN_INTERPOLATED_VELOCITY:
+            field("BC_VELOCITY", 3)[:, sel] = np.asarray(bc_values)[1:4, sel]
+        if kinds[k] == _abi.DYN_INTERPOLATED_PRESSURE:
+            field("RHO", 1)[0, sel] = np.asarray(bc_values)[0, sel]
+            field(pressure_velocity_field(d.direction, d.orientation), 3)[:, sel] = np.asarray(bc_values)[1:4, sel]
+    extra = tuple(k for k in values if k not in descriptor_fields)
+    return lattice_fields(q, tuple(descriptor_fields), extra), values
 
 
 def padded_shape(size, overlap: int) -> tuple[int, int, int]:
@@ -269,6 +294,6 @@ def save(path, core_fields: dict, q: int, size, periodic, dtype, overlap: int,
     Path(path).write_bytes(encode_fields(core_fields, q, size, periodic, dtype, overlap, fields))
 
 
-__all__ = ["FIELD_KEYS", "FieldSpec", "lattice_fields", "setup_fields", "encode", "decode", "file_name",
+__all__ = ["FIELD_KEYS", "FieldSpec", "field_key", "pressure_velocity_field", "lattice_fields", "setup_fields", "encode", "decode", "file_name",
            "parse_block", "write_block", "core_view", "pad_cells", "load_bytes", "encode_fields", "load", "save",
            "overlap_of"]

@@ -546,13 +546,13 @@ class SuperLattice:
     # -- checkpoints in OpenLB's format (openlb_b200/checkpoint.py) ----------
     def _checkpoint_fields(self, descriptor_fields):
         """The fields OpenLB's block would serialize for this set-up
-        (checkpoint.setup_fields over this lattice's dynamics table)."""
+        (checkpoint.setup_fields over this lattice's dynamics table and the
+        boundary values defineU / defineRho gave interpolated boundaries; with
+        inlet fluctuations on, those are the base values)."""
         from . import checkpoint as CK
-        if self._bc:
-            raise NotImplementedError("checkpoints of lattices with interpolated boundaries: their momenta "
-                                      "allocate one VELOCITY field per boundary normal")
         table, ids = self._table()
-        return CK.setup_fields(self.descriptor.q, ids, table, descriptor_fields)
+        return CK.setup_fields(self.descriptor.q, ids, table, descriptor_fields,
+                               bc_values=self._values() if self._bc else None)
 
     # Serializable::save(fileName) (core/serializer.hh:145-149), without the
     # log-directory prefix: writes <fileName>_rank0_size1.dat

@@ -84,33 +84,44 @@ def fixture_cases():
 
 def checkpoint_cases():
     """(name, case, initial state, steps before the save, steps after it, dtype,
-    descriptor fields, fields the set-up allocates) for the checkpoint fixtures."""
+    descriptor fields) for the checkpoint fixtures."""
     rng = np.random.default_rng(99)
     out = []
     case = C.periodic_case(19, (7, 6, 5), kind=O.BGK)
     out.append(("checkpoint_periodic_q19_float32_bgk", case, C.random_state(19, case.n, np.float32, rng),
-                5, 4, np.float32, ("FORCE",), ()))
+                5, 4, np.float32, ("FORCE",)))
     case = C.periodic_case(27, (6, 5, 4), kind=O.TRT)
     out.append(("checkpoint_periodic_q27_float64_trt", case, C.random_state(27, case.n, np.float64, rng),
-                3, 3, np.float64, ("FORCE",), ()))
+                3, 3, np.float64, ("FORCE",)))
     case = C.cavity_case(19, (9, 8, 7))
     out.append(("checkpoint_cavity_q19_float64", case, C.rest_state(19, case.n, np.float64),
-                12, 8, np.float64, ("FORCE",), ("VELOCITY", "RHO")))
+                12, 8, np.float64, ("FORCE",)))
     case = C.porous_case(19, (12, 9, 8), np.random.default_rng(7), g=1e-4)
     out.append(("checkpoint_porous_q19_float32", case, C.rest_state(19, case.n, np.float32),
-                10, 6, np.float32, ("FORCE",), ("RHO",)))
+                10, 6, np.float32, ("FORCE",)))
+    # interpolated velocity inlet / pressure outlet: momenta fields per boundary normal
+    case = C.interpolated_channel_case(19, (12, 8, 7), mixin=O.BGK, side=2, seed=5)
+    out.append(("checkpoint_interp_channel_q19_float32_bgk", case, C.rest_state(19, case.n, np.float32),
+                14, 10, np.float32, ("FORCE",)))
+    case = C.interpolated_channel_case(27, (10, 7, 6), mixin=O.SMAGORINSKY, side=0, seed=6)
+    out.append(("checkpoint_interp_channel_q27_float64_smagorinsky", case, C.rest_state(27, case.n, np.float64),
+                9, 7, np.float64, ("FORCE",)))
     return out
 
 
-def checkpoint_fixture(name, case, f0, steps, resume, dtype, dfields, efields):
+def checkpoint_fixture(name, case, f0, steps, resume, dtype, dfields):
     """OpenLB saves after `steps`; this library's file for that state is written
     and OpenLB resumes from it for `resume` steps, which must equal OpenLB's
     own run of steps + resume."""
-    fields = CK.lattice_fields(case.q, dfields, efields)
+    fields, setup = CK.setup_fields(case.q, case.dyn_id if case.dyn_id is not None else np.zeros(case.n, np.uint8),
+                                    case.table, dfields, case.bc_values)
     saved = O.run_reference(case, steps, dtype, init=f0, threads=1, save_checkpoint=True)
     arrays, overlap = CK.load_bytes(saved["checkpoint"], case.q, case.size, dtype, fields)
     if not np.array_equal(arrays["POPULATION"].reshape(-1), saved["pops"]):
         raise AssertionError(f"{name}: the file's populations differ from OpenLB's own dump")
+    for k, v in setup.items():
+        if not np.array_equal(v.astype(dtype), arrays[k]):
+            raise AssertionError(f"{name}: field {k} of the set-up differs from OpenLB's")
     ours = CK.encode_fields(arrays, case.q, case.size, case.periodic, dtype, overlap, fields)
     resumed = O.run_reference(case, resume, dtype, init=f0, threads=1, load_checkpoint=ours)
     straight = O.run_reference(case, steps + resume, dtype, init=f0, threads=1)
@@ -128,16 +139,21 @@ def checkpoint_fixture(name, case, f0, steps, resume, dtype, dfields, efields):
         "periodic": np.array(case.periodic, np.int32), "overlap": np.int32(overlap),
         "steps": np.int32(steps), "resume_steps": np.int32(resume),
         "dyn_id": case.dyn_id if case.dyn_id is not None else np.zeros(case.n, np.uint8),
-        "table": np.array([[d.kind, d.omega, d.magic, d.smagorinsky, *d.force, *d.wall_u, d.wall_rho]
-                           for d in case.table], np.float64),
-        "descriptor_fields": np.array(dfields, dtype="U16"), "extra_fields": np.array(efields, dtype="U16"),
+        "table": np.array([[d.kind, d.omega, d.magic, d.smagorinsky, *d.force, *d.wall_u, d.wall_rho,
+                            d.mixin, d.direction, d.orientation] for d in case.table], np.float64),
+        "descriptor_fields": np.array(dfields, dtype="U24"),
+        "extra_fields": np.array([f.name for f in fields if f.name != "POPULATION" and f.name not in dfields],
+                                 dtype="U24"),
         "init": f0, "pops_saved": saved["pops"], "pops_resumed": resumed["pops"],
         "checkpoint_ref": np.frombuffer(saved["checkpoint"], np.uint8),
         "checkpoint_ours": np.frombuffer(ours, np.uint8),
         # the oracle restates the generic templates: bit-identical except the
-        # CSE-generated D3Q19 BGK, which agrees to rounding
-        "tolerance": np.float64(2e-6 if dtype == np.float32 else 1e-13),
+        # CSE-generated D3Q19 BGK / Smagorinsky and the in-place boundary loop,
+        # which agree to rounding
+        "tolerance": np.float64(2e-6 if dtype == np.float32 else 1e-10),
     }
+    if case.bc_values is not None:
+        payload["bc_values"] = case.bc_values
     for k, v in arrays.items():
         if k != "POPULATION":
             payload[f"field_{k}"] = v
@@ -223,10 +239,10 @@ def main(only: str | None = None):
         manifest[name] = {"variant": variant, "dtype": np.dtype(dtype).name, "steps": steps,
                           "sha256": hashlib.sha256(path.read_bytes()).hexdigest()}
         print(name, path.stat().st_size)
-    for name, case, f0, steps, resume, dtype, dfields, efields in checkpoint_cases():
+    for name, case, f0, steps, resume, dtype, dfields in checkpoint_cases():
         if not wanted(name):
             continue
-        payload = checkpoint_fixture(name, case, f0, steps, resume, dtype, dfields, efields)
+        payload = checkpoint_fixture(name, case, f0, steps, resume, dtype, dfields)
         path = HERE / f"{name}.npz"
         np.savez_compressed(path, **payload)
         manifest[name] = {"variant": "sisd", "dtype": np.dtype(dtype).name, "steps": steps + resume,

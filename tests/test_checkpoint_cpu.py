@@ -22,6 +22,17 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 CASES = sorted(p.stem for p in GOLDEN.glob("checkpoint_*.npz"))
 
 
+def fixture_case(z):
+    """The fixture's set-up as an oracle case."""
+    from oracle import oracle as O
+    table = [O.Dynamics(int(r[0]), omega=r[1], magic=r[2], smagorinsky=r[3], force=tuple(r[4:7]),
+                        wall_u=tuple(r[7:10]), wall_rho=r[10], mixin=int(r[11]), direction=int(r[12]),
+                        orientation=int(r[13])) for r in z["table"]]
+    return O.Case(q=int(z["q"]), size=tuple(int(s) for s in z["size"]),
+                  periodic=tuple(int(p) for p in z["periodic"]), table=table, dyn_id=z["dyn_id"],
+                  bc_values=z["bc_values"] if "bc_values" in z.files else None)
+
+
 def test_file_text_is_two_padded_base64_streams():
     payload = bytes(range(7))
     text = CK.encode(payload)
@@ -39,9 +50,15 @@ def test_decode_rejects_a_size_mismatch():
 
 
 def test_field_order_follows_the_mangled_type_names():
-    names = [f.name for f in CK.lattice_fields(19, ("FORCE",), ("RHO", "VELOCITY"))]
-    assert names == ["POPULATION", "FORCE", "VELOCITY", "RHO"]
-    assert sorted(CK.FIELD_KEYS[n] for n in names) == [CK.FIELD_KEYS[n] for n in names]
+    names = [f.name for f in CK.lattice_fields(19, ("FORCE",), ("RHO", "VELOCITY", "BC_VELOCITY",
+                                                                "PRESSURE_VELOCITY_0-", "PRESSURE_VELOCITY_0+"))]
+    assert names == ["POPULATION", "FORCE", "VELOCITY", "RHO", "PRESSURE_VELOCITY_0+", "PRESSURE_VELOCITY_0-",
+                     "BC_VELOCITY"]
+    # FixedPressureMomentum<0,-1>: a negative template argument mangles as "n1"
+    assert CK.field_key("PRESSURE_VELOCITY_0-") == \
+        "N3olb5ArrayINS_7momenta21FixedPressureMomentumILi0ELin1EE8VELOCITYEEE"
+    with pytest.raises(ValueError):
+        CK.field_key("PRESSURE_VELOCITY_3+")
 
 
 def test_cyclic_columns_unroll_by_their_shift():
@@ -115,9 +132,7 @@ def test_openlb_resumes_from_our_checkpoint(name, oracle_mod):
     assert text == z["checkpoint_ours"].tobytes()
     # the oracle continues from the state read back exactly as OpenLB continued from the file
     arrays, _ = CK.load_bytes(text, q, size, dtype, fields)
-    table = [O.Dynamics(int(r[0]), omega=r[1], magic=r[2], smagorinsky=r[3], force=tuple(r[4:7]),
-                        wall_u=tuple(r[7:10]), wall_rho=r[10]) for r in z["table"]]
-    case = O.Case(q=q, size=size, periodic=periodic, table=table, dyn_id=z["dyn_id"])
+    case = fixture_case(z)
     pops = np.ascontiguousarray(arrays["POPULATION"].reshape(-1))
     O.step(case, pops, int(z["resume_steps"]))
     ref = z["pops_resumed"]
@@ -132,12 +147,11 @@ def test_openlb_resumes_from_our_checkpoint(name, oracle_mod):
 def test_setup_fields_match_openlbs(name):
     """The FORCE / VELOCITY / RHO values this library derives from a set-up are
     the ones OpenLB serialized for the same set-up."""
-    from oracle import oracle as O
     z = np.load(GOLDEN / f"{name}.npz")
     q = int(z["q"])
-    table = [O.Dynamics(int(r[0]), omega=r[1], magic=r[2], smagorinsky=r[3], force=tuple(r[4:7]),
-                        wall_u=tuple(r[7:10]), wall_rho=r[10]) for r in z["table"]]
-    fields, values = CK.setup_fields(q, z["dyn_id"], table, tuple(str(s) for s in z["descriptor_fields"]))
+    case = fixture_case(z)
+    fields, values = CK.setup_fields(q, z["dyn_id"], case.table, tuple(str(s) for s in z["descriptor_fields"]),
+                                     case.bc_values)
     assert [f.name for f in fields] == [f.name for f in CK.lattice_fields(
         q, tuple(str(s) for s in z["descriptor_fields"]), tuple(str(s) for s in z["extra_fields"]))]
     dtype = z["pops_saved"].dtype
