@@ -157,3 +157,21 @@ def test_setup_fields_match_openlbs(name):
     dtype = z["pops_saved"].dtype
     for k, v in values.items():
         np.testing.assert_array_equal(v.astype(dtype), z[f"field_{k}"])
+
+
+def test_truncated_or_foreign_files_are_rejected(tmp_path):
+    q, size = 19, (4, 3, 2)
+    pops = np.zeros((q, 24), np.float32)
+    text = CK.encode_fields({"POPULATION": pops}, q, size, (1, 1, 1), np.float32, 1)
+    payload = CK.decode(text)
+    with pytest.raises(ValueError, match="ends inside field POPULATION"):
+        CK.parse_block(payload[:-4], CK.lattice_fields(q), np.float32)
+    with pytest.raises(ValueError, match="does not pad"):
+        CK.load_bytes(text, q, (5, 3, 2), np.float32)
+    # a payload written with FP64 values read as FP32 leaves bytes over
+    with pytest.raises(ValueError):
+        CK.load_bytes(CK.encode_fields({"POPULATION": pops}, q, size, (1, 1, 1), np.float64, 1), q, size,
+                      np.float32)
+    bad = struct.pack("<q", 24) + struct.pack("<Q", 24) + bytes(96)
+    with pytest.raises(ValueError, match="shift 24 out of range"):
+        CK.parse_block(bad, [CK.FieldSpec("POPULATION", 1, cyclic=True)], np.float32)
