@@ -100,6 +100,15 @@ struct ResidualPartial {
 
 enum : int32_t { CELL_FLUID = 0, CELL_WALL = 1, CELL_LID = 2 };
 
+// flat-index offset of lattice vector (CX, CY, CZ) in a box with ny*nz = nynz
+// (modulo 2^32: negative components wrap, and n + offset is exact whenever the
+// neighbour lies inside the box)
+template <int CX, int CY, int CZ>
+OLB_DEV uint32_t flat_offset(uint32_t nynz, uint32_t nz)
+{
+  return uint32_t(CX) * nynz + uint32_t(CY) * nz + uint32_t(CZ);
+}
+
 OLB_DEV int cell_kind(const InstanceDevice& I, int x, int y, int z)
 {
   if (I.kind == OLB_B200_ENSEMBLE_CAVITY) {
@@ -138,11 +147,25 @@ ensemble_step_kernel(float* __restrict__ pool, const InstanceDevice* __restrict_
       const uint32_t z = r - y * I.nz_u;
       const int kind = cell_kind(I, int(x), int(y), int(z));
       if (kind == CELL_WALL) continue;  // full-way bounce-back: AA no-op
-      Neighbours nb(g, int(x), int(y), int(z));
+      // Odd steps address neighbours.  A cell off every face of its box reaches
+      // them without wrap-around: neighbour (x+cx, y+cy, z+cz) is the flat index
+      // n + cx*ny*nz + cy*nz + cz, so each population's address is n plus a
+      // per-instance constant.  Cells on a face (the lid row, the periodic x
+      // ends of a channel) take the wrap-around offsets.
+      const bool inner = (x - 1u < uint32_t(I.nx - 2)) && (y - 1u < uint32_t(I.ny - 2)) &&
+                         (z - 1u < uint32_t(I.nz - 2));
+      const uint32_t nynz = I.nynz, nzu = I.nz_u;
       float f[kQ];
       if (!odd) {
         static_for<0, kQ>([&](auto i) { f[i] = pops[uint32_t(i.value) * stride + n]; });
+      } else if (inner) {
+        static_for<0, kQ>([&](auto i) {
+          constexpr int o = L::opp(i);
+          f[i] = pops[n + (uint32_t(o) * stride +
+                           flat_offset<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>(nynz, nzu))];
+        });
       } else {
+        Neighbours nb(g, int(x), int(y), int(z));
         static_for<0, kQ>([&](auto i) {
           constexpr int o = L::opp(i);
           f[i] = pops[uint32_t(o) * stride + nb.template at<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>()];
@@ -176,7 +199,12 @@ ensemble_step_kernel(float* __restrict__ pool, const InstanceDevice* __restrict_
           constexpr int o = L::opp(i);
           pops[uint32_t(o) * st + n] = f[i];
         });
+      } else if (inner) {
+        static_for<0, kQ>([&](auto i) {
+          pops[n + (uint32_t(i.value) * st + flat_offset<L::c(i, 0), L::c(i, 1), L::c(i, 2)>(nynz, nzu))] = f[i];
+        });
       } else {
+        Neighbours nb(g, int(x), int(y), int(z));
         static_for<0, kQ>([&](auto i) {
           pops[uint32_t(i.value) * st + nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>()] = f[i];
         });
