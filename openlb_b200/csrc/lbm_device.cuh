@@ -753,20 +753,30 @@ OLB_DEV float smagorinsky_omega_scaled(const float (&g)[L::q], float rho, float 
 }
 
 // Guo forcing (lbm::addExternalForce, src/dynamics/lbm.h:544-566) on g: the
-// term of population i scaled by s_i (folded into s_i t_i)
+// term of population i, t_i (3 (c_i - u).F + 9 (c_i.u)(c_i.F)) force_relax rho,
+// scaled by s_i (folded into s_i t_i).  Over an opposite pair c_opp = -c_i the
+// two terms are A + B and A - B with A = 9 (c_i.u)(c_i.F) - 3 u.F and
+// B = 3 c_i.F, so each pair costs two dot products with entries of +-1.
 template <class L>
 OLB_DEV void add_force_scaled(float (&g)[L::q], float rho, const float (&u)[3], float force_relax,
                               const float (&gf)[3])
 {
-  static_for<0, L::q>([&](auto i) {
+  const float fr = force_relax * rho;
+  const float uf3 = 3.f * (u[0] * gf[0] + u[1] * gf[1] + u[2] * gf[2]);
+  {
+    constexpr float T = storage_scale<L>(0) * weight<L, float>(0);
+    g[0] -= uf3 * (T * fr);
+  }
+  static_for<1, L::half + 1>([&](auto i) {
+    constexpr int o = L::opp(i);
     constexpr float T = storage_scale<L>(i) * weight<L, float>(i);
-    const float cu = 9.f * c_dot<L, i.value>(u);
-    float term = 0.f;
-    static_for<0, 3>([&](auto d) {
-      constexpr int cc = L::c(i, d);
-      term += ((float(cc) - u[d]) * 3.f + cu * float(cc)) * gf[d];
-    });
-    g[i] += term * (T * force_relax * rho);
+    const float cu = c_dot<L, i.value>(u);
+    const float cf = c_dot<L, i.value>(gf);
+    const float a = 9.f * cu * cf - uf3;
+    const float b = 3.f * cf;
+    const float k = T * fr;
+    g[i] += (a + b) * k;
+    g[o] += (a - b) * k;
   });
 }
 

@@ -195,6 +195,28 @@ def test_16bit_storage_velocity_error(storage, bound):
     assert err <= bound, err
 
 
+@pytest.mark.parametrize("kind", [O.TRT, O.FORCED_TRT], ids=["trt", "forced_trt"])
+@pytest.mark.parametrize("storage,bound", [("f16", 1e-3), ("bf16", 5e-3)])
+def test_16bit_trt_velocity_error(kind, storage, bound):
+    """TRT and Guo-forced TRT on the scaled 16-bit representation: velocity L2
+    after 200 steps vs the FP64 oracle, with the FP16/BF16 bounds above."""
+    q = 19
+    size = (24, 24, 24)
+    n = np.prod(size)
+    x = (np.arange(size[0]) + 0.5) * 2 * np.pi / size[0]
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    u0 = 0.05
+    u = np.stack([u0 * np.sin(X) * np.cos(Y) * np.cos(Z), -u0 * np.cos(X) * np.sin(Y) * np.cos(Z),
+                  np.zeros_like(X)]).reshape(3, -1)
+    case = C.periodic_case(q, size, kind=kind, omega=1 / (0.5 + 3 * 0.0125), force=(1e-5, -2e-6, 3e-6))
+    f0_64 = O.equilibrium(q, np.ones(n), u)
+    ref, _ = run_oracle(case, f0_64, 200)
+    _, r_u = O.moments(case, ref)
+    got, _, gu, _ = run_gpu(case, f0_64.astype(np.float32), 200, storage=storage)
+    err = np.linalg.norm(gu - r_u) / np.linalg.norm(r_u)
+    assert err <= bound, err
+
+
 def test_set_populations_resets_layout():
     """Upload after an odd number of steps: the AA parity is internal."""
     rng = np.random.default_rng(3)
