@@ -378,9 +378,9 @@ OLB_DEV void relax_trt(R (&f)[L::q], R rho, R delta, const R (&u)[3], R omega, R
 #endif
 }
 
-// lbm::addExternalForce (Guo)  src/dynamics/lbm.h:544-566
+// lbm::addExternalForce (Guo)  src/dynamics/lbm.h:544-566, reference operation order
 template <class L, class R>
-OLB_DEV void add_force(R (&f)[L::q], R rho, const R (&u)[3], R force_relax, const R (&g)[3])
+OLB_DEV void add_force_reference(R (&f)[L::q], R rho, const R (&u)[3], R force_relax, const R (&g)[3])
 {
   constexpr R inv_cs2 = R(3);
   static_for<0, L::q>([&](auto i) {
@@ -397,6 +397,39 @@ OLB_DEV void add_force(R (&f)[L::q], R rho, const R (&u)[3], R force_relax, cons
     term *= rho;
     f[i] += term;
   });
+}
+
+// The same force terms over opposite pairs: with c_opp = -c_i the terms of i
+// and opp(i) are t_i (A + B) and t_i (A - B) times force_relax rho, where
+// A = 9 (c_i.u)(c_i.F) - 3 u.F and B = 3 c_i.F (reassociated: agrees with the
+// reference order to rounding).
+template <class L, class R>
+OLB_DEV void add_force_paired(R (&f)[L::q], R rho, const R (&u)[3], R force_relax, const R (&g)[3])
+{
+  const R fr = force_relax * rho;
+  const R uf3 = R(3) * (u[0] * g[0] + u[1] * g[1] + u[2] * g[2]);
+  f[0] -= uf3 * (weight<L, R>(0) * fr);
+  static_for<1, L::half + 1>([&](auto i) {
+    constexpr int o = L::opp(i);
+    constexpr R t = weight<L, R>(i);
+    const R cu = c_dot<L, i.value>(u);
+    const R cf = c_dot<L, i.value>(g);
+    const R a = R(9) * cu * cf - uf3;
+    const R b = R(3) * cf;
+    const R k = t * fr;
+    f[i] += (a + b) * k;
+    f[o] += (a - b) * k;
+  });
+}
+
+template <class L, class R>
+OLB_DEV void add_force(R (&f)[L::q], R rho, const R (&u)[3], R force_relax, const R (&g)[3])
+{
+#ifdef OLB_B200_EXACT
+  add_force_reference<L>(f, rho, u, force_relax, g);
+#else
+  add_force_paired<L>(f, rho, u, force_relax, g);
+#endif
 }
 
 // |Pi_neq|^2 for bulk momenta: lbm::computeStress (lbm.h:310-329) and the
