@@ -200,6 +200,17 @@ olb_b200_status olb_b200_get_moments(olb_b200_lattice* lattice, void* host_rho, 
 /* Waits for all work enqueued on the lattice. */
 olb_b200_status olb_b200_synchronize(olb_b200_lattice* lattice);
 
+/* Bounds the pipeline of olb_b200_collide_and_stream calls without
+ * statistics: with calls = n > 0, a call first waits until the device work of
+ * the call issued n calls earlier has finished, so at most n calls are
+ * pending on the device when it returns; 0 (the default) leaves the queue
+ * unbounded.  A host that times steps with a wall clock, as OpenLB's
+ * util::Timer does (src/utilities/timer.hh:36-76), then measures device time
+ * to within n steps, while the device is never left idle between steps.  The
+ * reference's GPU platform instead synchronises the device three times per
+ * step (src/core/superLattice.hh:669-671).  Waits for pending work first. */
+olb_b200_status olb_b200_set_max_steps_in_flight(olb_b200_lattice* lattice, int32_t calls);
+
 /* Device time of `steps` collide-and-stream steps, measured with CUDA events
  * on the lattice's stream (synchronous). */
 olb_b200_status olb_b200_time_steps(olb_b200_lattice* lattice, int32_t steps, float* milliseconds);
@@ -245,21 +256,34 @@ olb_b200_status olb_b200_set_step_variant(olb_b200_lattice* lattice, int32_t var
  * cudaFree outside it, or a service that sizes its memory once at start-up and
  * must not allocate on the request path.  No lattice handle is involved (the
  * handle allocates); the caller owns the populations:
+ *   desc         periodic must be {1,1,1}: every axis wraps (a lattice with
+ *                walls needs a handle); reserved must be 0; nx <= 65535.
  *   device_pops  q columns of stride = round_up(nx*ny*nz, 64) elements of the
  *                storage type, in this library's in-place (AA) order: after an
  *                even number of steps it is the logical post-stream layout,
  *                after an odd number each f_i(x) sits in column opp(i) at
  *                x - c_i.  steps_done tells the call which of the two it is.
+ *                One cell per element in every storage (the natural layout;
+ *                a handle's paired 16-bit layout is not used here).  F32 and
+ *                F64 hold f_i - w_i.  F16 and BF16 hold (f_i - w_i) * s_i
+ *                rounded to the 16-bit type, s_i the power of two nearest
+ *                1/w_i (s/sqrt2 < 1/w_i <= s*sqrt2): D3Q19 s = 4 (rest), 16
+ *                (axis), 32 (diagonal); D3Q27 s = 4, 16, 64 (edge), 256
+ *                (corner).
  *   bulk         one fluid dynamics applied to every cell (no walls).
  *   stats        NULL, or receives the last step's statistics (the call then
  *                waits for the stream).
  *   stream       a cudaStream_t, or NULL for the default stream.
  * The statistics reduction uses a fixed 2.5 MiB __device__ scratch array that
- * every GPU loading this library holds until exit; lattices needing more than
- * 65536 reduction blocks (more than 256^3 cells) are rejected with
- * OLB_B200_ERR_ARG when stats is requested.  The first call on each device
- * looks up the scratch address and should come before any stream capture.
- * Calls whose device work overlaps race on the shared scratch; serialise them. */
+ * every GPU loading this library holds until exit.  With stats requested the
+ * call needs ceil(nz/bz) * ceil(ny/by) * nx reduction blocks, (bz, by) =
+ * (128, 2) if nz >= 128, (64, 4) if nz >= 64, else (32, 8); more than 65536
+ * (e.g. any lattice above 256^3 cells) is rejected with OLB_B200_ERR_ARG.
+ * The first call on each device looks up the scratch address and keeps it:
+ * it should come before any stream capture, and the kept address is stale
+ * after cudaDeviceReset on that device.  Calls whose device work overlaps
+ * (two threads, two streams) race on the shared scratch: the caller
+ * serialises them. */
 olb_b200_status olb_b200_collide_and_stream_noalloc(const olb_b200_desc* desc, void* device_pops,
                                                     int64_t steps_done,
                                                     const olb_b200_dyn_params* bulk, int32_t steps,

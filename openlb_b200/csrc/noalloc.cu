@@ -60,8 +60,10 @@ using namespace olb_b200;
 namespace {
 
 // Scratch for the per-block statistics partials plus one slot for the reduced
-// result: (65536 + 1) * 40 B = 2.5 MiB per device.  65536 blocks cover a
-// 256 x 256 x 256 lattice with the default launch shape.
+// result: (65536 + 1) * 40 B = 2.5 MiB per device.  A call with statistics
+// launches ceil(nz/bz) * ceil(ny/by) * nx blocks, (bz, by) = (128, 2) for
+// nz >= 128, (64, 4) for nz >= 64, else (32, 8): 65536 blocks cover a
+// 256 x 256 x 256 lattice, but only 2048 x 256 x 16 for a thin one.
 constexpr size_t kMaxBlocks = 65536;
 static __device__ __align__(256) StatPartial g_noalloc_scratch[kMaxBlocks + 1];
 
@@ -80,7 +82,10 @@ olb_b200_status noalloc_cuda(cudaError_t e, const char* what)
   return noalloc_fail(OLB_B200_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-// Device address of the scratch array on `device` (the current device).
+// Device address of the scratch array on `device` (the current device),
+// looked up on the first call on that device and kept for the process: after
+// cudaDeviceReset on that device the kept address is stale, so callers that
+// reset a device must not use this entry point on it afterwards.
 olb_b200_status scratch_address(int device, StatPartial** out)
 {
   std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -105,6 +110,16 @@ extern "C" olb_b200_status olb_b200_collide_and_stream_noalloc(
   if (desc->q != 19 && desc->q != 27) return noalloc_fail(OLB_B200_ERR_ARG, "collide_and_stream_noalloc: q must be 19 or 27");
   if (desc->nx < 1 || desc->ny < 1 || desc->nz < 1 || desc->storage < 0 || desc->storage > 3)
     return noalloc_fail(OLB_B200_ERR_ARG, "collide_and_stream_noalloc: invalid lattice description");
+  if (desc->reserved[0] || desc->reserved[1] || desc->reserved[2])
+    return noalloc_fail(OLB_B200_ERR_ARG, "collide_and_stream_noalloc: reserved fields must be zero");
+  // the step grid puts x in gridDim.z
+  if (desc->nx > 65535) return noalloc_fail(OLB_B200_ERR_ARG, "collide_and_stream_noalloc: nx exceeds 65535");
+  // One bulk dynamics and no walls: the step wraps every axis.  A box with
+  // closed faces needs wall cells (per-cell dynamics), which only a lattice
+  // handle carries.
+  if (desc->periodic[0] != 1 || desc->periodic[1] != 1 || desc->periodic[2] != 1)
+    return noalloc_fail(OLB_B200_ERR_ARG, "collide_and_stream_noalloc: every axis must be periodic "
+                        "(periodic = {1,1,1}); lattices with walls need a lattice handle");
   if (desc->device < 0 || desc->device >= kMaxDevices)
     return noalloc_fail(OLB_B200_ERR_ARG, "collide_and_stream_noalloc: device ordinal out of range");
   if (steps < 1 || steps_done < 0) return noalloc_fail(OLB_B200_ERR_ARG, "collide_and_stream_noalloc: steps must be >= 1");
@@ -124,8 +139,9 @@ extern "C" olb_b200_status olb_b200_collide_and_stream_noalloc(
   const size_t blocks = size_t(grid.x) * grid.y * grid.z;
   if (stats && blocks > kMaxBlocks) {
     char buf[256];
-    snprintf(buf, sizeof buf, "collide_and_stream_noalloc: lattice needs %zu statistics blocks; the "
-             "fixed scratch holds %zu (at most 256x256x256 cells)", blocks, kMaxBlocks);
+    snprintf(buf, sizeof buf, "collide_and_stream_noalloc: with statistics the lattice needs "
+             "ceil(nz/%d)*ceil(ny/%d)*nx = %zu reduction blocks; the fixed scratch holds %zu",
+             bz, by, blocks, kMaxBlocks);
     return noalloc_fail(OLB_B200_ERR_ARG, buf);
   }
 

@@ -283,6 +283,10 @@ struct olb_b200_lattice {
   double noise_amp = 0.0;           // inlet fluctuations (olb_b200_set_boundary_noise)
   uint64_t noise_seed = 0;
   bool initialized = false;         // PostStream post-processors applied to the initial state
+  // bounded pipeline of collide_and_stream calls (olb_b200_set_max_steps_in_flight)
+  std::vector<cudaEvent_t> flight;  // ring: event after the call k - flight.size()
+  std::vector<bool> flight_used;
+  size_t flight_pos = 0;
 };
 
 namespace {
@@ -652,6 +656,7 @@ void olb_b200_destroy(olb_b200_lattice* L)
   if (L->stat_host) cudaFreeHost(L->stat_host);
   if (L->ev0) cudaEventDestroy(L->ev0);
   if (L->ev1) cudaEventDestroy(L->ev1);
+  for (cudaEvent_t e : L->flight) cudaEventDestroy(e);
   if (L->stream) cudaStreamDestroy(L->stream);
   delete L;
 }
@@ -838,8 +843,18 @@ olb_b200_status olb_b200_collide_and_stream(olb_b200_lattice* L, int32_t steps, 
   }
   st = initialize_once(L);
   if (st != OLB_B200_OK) return st;
+  const bool bounded = !stats && !L->flight.empty();
+  if (bounded && L->flight_used[L->flight_pos]) {
+    // wait for the call issued flight.size() calls ago
+    OLB_CUDA(cudaEventSynchronize(L->flight[L->flight_pos]));
+  }
   st = enqueue_steps(L, steps, stats != nullptr);
   if (st != OLB_B200_OK) return st;
+  if (bounded) {
+    OLB_CUDA(cudaEventRecord(L->flight[L->flight_pos], L->stream));
+    L->flight_used[L->flight_pos] = true;
+    L->flight_pos = (L->flight_pos + 1) % L->flight.size();
+  }
   if (!stats) return OLB_B200_OK;
   const dim3 grid = step_grid(L->g, L->block_z, L->block_y, cells_per_thread(L));
   const size_t count = size_t(grid.x) * grid.y * grid.z;
@@ -908,6 +923,22 @@ olb_b200_status olb_b200_time_steps(olb_b200_lattice* L, int32_t steps, float* m
   OLB_CUDA(cudaEventRecord(L->ev1, L->stream));
   OLB_CUDA(cudaEventSynchronize(L->ev1));
   OLB_CUDA(cudaEventElapsedTime(ms, L->ev0, L->ev1));
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_set_max_steps_in_flight(olb_b200_lattice* L, int32_t calls)
+{
+  g_last_error.clear();
+  if (!L) return fail(OLB_B200_ERR_ARG, "set_max_steps_in_flight: null lattice");
+  if (calls < 0 || calls > 64) return fail(OLB_B200_ERR_ARG, "set_max_steps_in_flight: %d not in [0, 64]", calls);
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  for (cudaEvent_t e : L->flight) cudaEventDestroy(e);
+  L->flight.assign(size_t(calls), nullptr);
+  L->flight_used.assign(size_t(calls), false);
+  L->flight_pos = 0;
+  for (cudaEvent_t& e : L->flight) OLB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   return OLB_B200_OK;
 }
 

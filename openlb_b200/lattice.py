@@ -273,6 +273,10 @@ class Lattice:
     def synchronize(self) -> None:
         self._check(self._lib.olb_b200_synchronize(self._h))
 
+    def set_max_steps_in_flight(self, calls: int) -> None:
+        """At most `calls` collide_and_stream calls pending on the device (0: unbounded)."""
+        self._check(self._lib.olb_b200_set_max_steps_in_flight(self._h, int(calls)))
+
     def velocity_residual(self) -> float:
         """||u - u_prev|| / ||u|| over fluid cells since the previous call."""
         r = ctypes.c_double()
