@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define OLB_B200_ABI_VERSION 2
+#define OLB_B200_ABI_VERSION 3
 
 typedef struct olb_b200_lattice olb_b200_lattice;
 
@@ -72,7 +72,18 @@ typedef enum {
    * mixin dynamics with exchanged momenta, plus PlaneFdBoundaryProcessor3D in
    * the PostStream stage (src/boundary/boundaryPostProcessors3D.hh:39-92). */
   OLB_B200_DYN_INTERPOLATED_VELOCITY = 8, /* boundary::InterpolatedVelocity  src/boundary/interpolatedVelocity3D.h:44-81 */
-  OLB_B200_DYN_INTERPOLATED_PRESSURE = 9  /* boundary::InterpolatedPressure  src/boundary/interpolatedPressure3D.h:47-90 */
+  OLB_B200_DYN_INTERPOLATED_PRESSURE = 9, /* boundary::InterpolatedPressure  src/boundary/interpolatedPressure3D.h:47-90 */
+  /* Local velocity boundary on a flat face: CombinedRLBdynamics<MIXIN,
+   * momenta::RegularizedVelocityBoundaryTuple<direction,orientation>>
+   * (src/dynamics/dynamics.h:394-437), no post-processor. */
+  OLB_B200_DYN_LOCAL_VELOCITY = 10,       /* boundary::LocalVelocity (flat)  src/boundary/localVelocity3D.h:47-80 */
+  /* External edges and corners of velocity boundaries (local and
+   * interpolated): MIXIN::exchange_momenta<momenta::FixedVelocityBoundaryTuple>
+   * plus OuterVelocityEdgeProcessor3D / OuterVelocityCornerProcessor3D in the
+   * PostStream stage (src/boundary/boundaryPostProcessors3D.hh:164-292);
+   * `normal` holds the discrete normal. */
+  OLB_B200_DYN_VELOCITY_EDGE = 11,        /* src/boundary/localVelocity3D.h:90-93,113-114 */
+  OLB_B200_DYN_VELOCITY_CORNER = 12       /* src/boundary/localVelocity3D.h:82-85,111-112 */
 } olb_b200_dyn_kind;
 
 typedef struct {
@@ -92,14 +103,18 @@ typedef struct {
  *   force        descriptors::FORCE field value (Guo forcing, forcing.h:38-74)
  *   wall_u       descriptors::VELOCITY field of BounceBackVelocity (defineU)
  *   wall_rho     FixedDensity RHO field (1 unless defineRho)
- * Interpolated boundary entries also carry
- *   mixin        the MixinDynamics template argument of boundary::Interpolated*
- *                (BGK, TRT or SMAGORINSKY; must be the lattice's fluid collision)
- *   direction,   the discrete normal of the face as the boundary setter derives
+ * Boundary entries (interpolated, local velocity, edges, corners) also carry
+ *   mixin        the MixinDynamics template argument of the boundary setter
+ *                (BGK, TRT or SMAGORINSKY; must be the lattice's fluid
+ *                collision; local velocity faces take BGK or TRT)
+ *   direction,   flat faces: the discrete normal as the boundary setter derives
  *   orientation  it (src/boundary/setBoundary3D.h:204-227): axis 0..2 and the
- *                sign of the outward normal, -1 or +1.  All cells of one entry
- *                should lie in one plane: their boundary values are stored over
- *                the bounding box of the entry's cells. */
+ *                sign of the outward normal, -1 or +1
+ *   normal       edges and corners: the discrete normal (each component -1, 0
+ *                or +1; two nonzero for an edge, three for a corner), as
+ *                promiseForNormalSpecial maps it (setBoundary3D.h:586-627)
+ * The boundary values of an entry's cells are stored over the bounding box of
+ * those cells: keep each entry's cells in one plane (one line for an edge). */
 typedef struct {
   int32_t kind;         /* olb_b200_dyn_kind */
   int32_t mixin;        /* olb_b200_dyn_kind of the mixin (interpolated boundaries), else 0 */
@@ -109,8 +124,10 @@ typedef struct {
   double force[3];
   double wall_u[3];
   double wall_rho;
-  int32_t direction;    /* interpolated boundaries: normal axis */
-  int32_t orientation;  /* interpolated boundaries: normal sign */
+  int32_t direction;    /* flat boundaries: normal axis */
+  int32_t orientation;  /* flat boundaries: normal sign */
+  int32_t normal[3];    /* edges and corners: discrete normal */
+  int32_t reserved;     /* must be 0 */
 } olb_b200_dyn_params;
 
 /* Statistics of one step as OpenLB's LatticeStatistics reports them

@@ -8,7 +8,8 @@ from . import _abi, boundary
 from .descriptors import D3Q19, D3Q27, Descriptor, descriptor
 from .lattice import (BGKdynamics, BounceBack, BounceBackVelocity, Dynamics, ForcedBGKdynamics,
                       ForcedTRTdynamics, InterpolatedPressureBoundary, InterpolatedVelocityBoundary, Lattice,
-                      NoDynamics, SmagorinskyBGKdynamics, SuperGeometry, SuperLattice, TRTdynamics)
+                      LocalVelocityBoundary, NoDynamics, SmagorinskyBGKdynamics, SuperGeometry, SuperLattice,
+                      TRTdynamics, VelocityCornerBoundary, VelocityEdgeBoundary)
 
 OlbError = _abi.OlbError
 Diverged = _abi.Diverged
@@ -26,7 +27,8 @@ def build_info() -> str:
 __all__ = [
     "D3Q19", "D3Q27", "Descriptor", "descriptor", "Dynamics", "NoDynamics", "BGKdynamics",
     "TRTdynamics", "ForcedTRTdynamics", "ForcedBGKdynamics", "SmagorinskyBGKdynamics", "BounceBack",
-    "BounceBackVelocity", "InterpolatedVelocityBoundary", "InterpolatedPressureBoundary", "boundary",
+    "BounceBackVelocity", "InterpolatedVelocityBoundary", "InterpolatedPressureBoundary",
+    "LocalVelocityBoundary", "VelocityEdgeBoundary", "VelocityCornerBoundary", "boundary",
     "Lattice", "SuperGeometry", "SuperLattice", "OlbError", "Diverged",
     "LibraryNotBuilt", "library_path", "build_info",
 ]

@@ -30,9 +30,13 @@ STORAGE = {"f32": 0, "f64": 1, "f16": 2, "bf16": 3}
 
 # dynamics kinds (olb_b200_dyn_kind)
 DYN_NONE, DYN_BGK, DYN_TRT, DYN_SMAGORINSKY, DYN_BOUNCE_BACK, DYN_BOUNCE_BACK_VELOCITY, \
-    DYN_FORCED_BGK, DYN_FORCED_TRT, DYN_INTERPOLATED_VELOCITY, DYN_INTERPOLATED_PRESSURE = range(10)
+    DYN_FORCED_BGK, DYN_FORCED_TRT, DYN_INTERPOLATED_VELOCITY, DYN_INTERPOLATED_PRESSURE, \
+    DYN_LOCAL_VELOCITY, DYN_VELOCITY_EDGE, DYN_VELOCITY_CORNER = range(13)
 DYN_INTERPOLATED = (DYN_INTERPOLATED_VELOCITY, DYN_INTERPOLATED_PRESSURE)
-ABI_VERSION = 2
+# boundary kinds whose cells carry values (RHO, VELOCITY) set by set_boundary_values
+DYN_VALUED = (DYN_INTERPOLATED_VELOCITY, DYN_INTERPOLATED_PRESSURE, DYN_LOCAL_VELOCITY,
+              DYN_VELOCITY_EDGE, DYN_VELOCITY_CORNER)
+ABI_VERSION = 3
 
 EXPORTED = [
     "olb_b200_create", "olb_b200_destroy", "olb_b200_set_dynamics", "olb_b200_set_populations",
@@ -79,7 +83,8 @@ class DynParams(ctypes.Structure):
                 ("omega", ctypes.c_double), ("magic", ctypes.c_double),
                 ("smagorinsky", ctypes.c_double), ("force", ctypes.c_double * 3),
                 ("wall_u", ctypes.c_double * 3), ("wall_rho", ctypes.c_double),
-                ("direction", ctypes.c_int32), ("orientation", ctypes.c_int32)]
+                ("direction", ctypes.c_int32), ("orientation", ctypes.c_int32),
+                ("normal", ctypes.c_int32 * 3), ("reserved", ctypes.c_int32)]
 
 
 class Stats(ctypes.Structure):

@@ -36,7 +36,16 @@ struct Geometry {
   int32_t nx, ny, nz;
   uint32_t stride;  // column length in storage elements
   int32_t paired;   // 1: 16-bit storage with cells x and x + nx/2 in one 4-byte element
+  // masked lattices: a box [lo, hi) whose cells all use the bulk entry, so the
+  // step kernel skips their dynamics id (empty when lo == hi)
+  int32_t bulk_lo[3], bulk_hi[3];
 };
+
+OLB_HD bool in_bulk_box(const Geometry& g, int x, int y, int z)
+{
+  return x >= g.bulk_lo[0] && x < g.bulk_hi[0] && y >= g.bulk_lo[1] && y < g.bulk_hi[1] && z >= g.bulk_lo[2] &&
+         z < g.bulk_hi[2];
+}
 
 // Scalar slot of a cell within a population column.
 //   natural layout: (x*ny + y)*nz + z
@@ -218,22 +227,30 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict
   R f[CPT][Q];
   int kind[CPT];
   bool go[CPT];
+  bool inside[CPT];  // masked lattices: in the bulk box, no dynamics id needed
   uint32_t n[CPT];
   const DynDevice<R>* p[CPT];
 
-  // phase 1: classify the cells and issue all their loads
+  // phase 1: classify the cells and issue all their loads.  Cells of the bulk
+  // box (all cells of an unmasked lattice) need no dynamics id: a warp whose
+  // cells all lie in the box issues its population loads at once, the others
+  // wait for their ids and kinds (full-way bounce-back moves no bytes).
   static_for<0, CPT>([&](auto k) {
     const int y = y0 + k.value * int(blockDim.y);
     go[k] = z < g.nz && y < g.ny;
     kind[k] = KIND;
-    p[k] = &bulk;
+    p[k] = nullptr;  // masked lattices: the cell's table entry (box cells use `bulk`)
     n[k] = 0;
+    inside[k] = !MASKED;
     if (go[k]) {
       n[k] = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
       if constexpr (MASKED) {
-        const DynDevice<R>* e = table + ids[n[k]];
-        kind[k] = __ldg(&e->kind);
-        p[k] = e;
+        inside[k] = in_bulk_box(g, x, y, z);
+        if (!inside[k]) {
+          const DynDevice<R>* e = table + ids[n[k]];
+          kind[k] = __ldg(&e->kind);
+          p[k] = e;
+        }
       }
       // full-way bounce-back is a no-op on the AA pattern (see file comment)
       go[k] = kind[k] != K_BOUNCE_BACK;
@@ -260,16 +277,28 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict
     bool counted = false;
     if (kind[k] == KIND) {
       if constexpr (MASKED) {
-        const DynDevice<R>* e = p[k];
+        // the entry's collision constants: the bulk entry's for box cells
         DynDevice<R> q;
-        q.omega = __ldg(&e->omega);
-        q.omega_minus = __ldg(&e->omega_minus);
-        q.smago_pre = __ldg(&e->smago_pre);
-        q.tau_mol = __ldg(&e->tau_mol);
-        q.force[0] = __ldg(&e->force[0]);
-        q.force[1] = __ldg(&e->force[1]);
-        q.force[2] = __ldg(&e->force[2]);
-        q.force_relax = __ldg(&e->force_relax);
+        if (inside[k]) {
+          q.omega = bulk.omega;
+          q.omega_minus = bulk.omega_minus;
+          q.smago_pre = bulk.smago_pre;
+          q.tau_mol = bulk.tau_mol;
+          q.force[0] = bulk.force[0];
+          q.force[1] = bulk.force[1];
+          q.force[2] = bulk.force[2];
+          q.force_relax = bulk.force_relax;
+        } else {
+          const DynDevice<R>* e = p[k];
+          q.omega = __ldg(&e->omega);
+          q.omega_minus = __ldg(&e->omega_minus);
+          q.smago_pre = __ldg(&e->smago_pre);
+          q.tau_mol = __ldg(&e->tau_mol);
+          q.force[0] = __ldg(&e->force[0]);
+          q.force[1] = __ldg(&e->force[1]);
+          q.force[2] = __ldg(&e->force[2]);
+          q.force_relax = __ldg(&e->force_relax);
+        }
         collide_bulk<L, KIND>(f[k], q, st_rho, st_usqr);
       } else {
         collide_bulk<L, KIND>(f[k], bulk, st_rho, st_usqr);
@@ -287,13 +316,10 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict
       const R wu[3] = {__ldg(&e->wall_u[0]), __ldg(&e->wall_u[1]), __ldg(&e->wall_u[2])};
       st_usqr = norm_sqr(wu);
       counted = true;
-    } else if (MASKED && is_interpolated(kind[k])) {
-      if constexpr (KIND == K_BGK || KIND == K_TRT || KIND == K_SMAGORINSKY) {
-        collide_interpolated<L, KIND>(f[k], kind[k], p[k], x, y, z, st_rho, st_usqr);
-        counted = true;
-      }
     }
-    // NoDynamics (and anything else): populations pass through unchanged.
+    // NoDynamics and the boundary cells that carry values (their collision
+    // ran in place before this kernel, boundary_collide_kernel): populations
+    // pass through unchanged.
     // The store offsets are recomputed here rather than kept live through
     // the collision.
     Neighbours nb(g, int(opaque(uint32_t(x))), int(opaque(uint32_t(y))), int(opaque(uint32_t(z))));
@@ -393,7 +419,7 @@ OLB_DEV bool collide_any(float (&f)[L::q], int kind, const DynDevice<float>* e, 
                          int x, int y, int z, float& st_rho, float& st_usqr)
 {
   if (kind == KIND) {
-    if constexpr (MASKED) {
+    if (MASKED && e) {
       DynDevice<float> q;
       q.omega = __ldg(&e->omega);
       q.omega_minus = __ldg(&e->omega_minus);
@@ -423,14 +449,9 @@ OLB_DEV bool collide_any(float (&f)[L::q], int kind, const DynDevice<float>* e, 
       const float wu[3] = {__ldg(&e->wall_u[0]), __ldg(&e->wall_u[1]), __ldg(&e->wall_u[2])};
       st_usqr = norm_sqr(wu);
       return true;
-    } else if (is_interpolated(kind)) {
-      if constexpr (KIND == K_BGK || KIND == K_TRT || KIND == K_SMAGORINSKY) {
-        collide_interpolated<L, KIND>(f, kind, e, x, y, z, st_rho, st_usqr);
-        return true;
-      }
     }
   }
-  return false;  // NoDynamics / bounce-back: no statistic
+  return false;  // NoDynamics / bounce-back / boundary cells (collided ahead): no statistic here
 }
 
 template <int Q, class S, int KIND, bool ODD, bool MASKED, bool STATS, int CPT, int MINB>
@@ -465,15 +486,18 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
     const int y = y0 + k.value * int(blockDim.y);
     go[k] = z < g.nz && y < g.ny;
     kind_lo[k] = kind_hi[k] = KIND;
-    p_lo[k] = p_hi[k] = &bulk;
+    p_lo[k] = p_hi[k] = nullptr;  // nullptr: the bulk entry (kernel argument)
     e[k] = 0;
     if (go[k]) {
       e[k] = (uint32_t(xp) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
       if constexpr (MASKED) {
-        p_lo[k] = table + ids[e[k]];
-        p_hi[k] = table + ids[e[k] + half_cells];
-        kind_lo[k] = __ldg(&p_lo[k]->kind);
-        kind_hi[k] = __ldg(&p_hi[k]->kind);
+        // both cells in the bulk box: the bulk entry, no dynamics ids
+        if (!(in_bulk_box(g, xp, y, z) && in_bulk_box(g, xp + (g.nx >> 1), y, z))) {
+          p_lo[k] = table + ids[e[k]];
+          p_hi[k] = table + ids[e[k] + half_cells];
+          kind_lo[k] = __ldg(&p_lo[k]->kind);
+          kind_hi[k] = __ldg(&p_hi[k]->kind);
+        }
       }
       // two bounce-back cells: nothing to do (AA no-op)
       go[k] = !(kind_lo[k] == K_BOUNCE_BACK && kind_hi[k] == K_BOUNCE_BACK);
@@ -525,7 +549,7 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
       bool counted = false, done = false;
 #ifndef OLB_B200_EXACT
       if (!MASKED || kind == KIND) {
-        if constexpr (MASKED) {
+        if (MASKED && pe) {
           DynDevice<float> q;
           q.omega = __ldg(&pe->omega);
           q.omega_minus = __ldg(&pe->omega_minus);
@@ -691,10 +715,17 @@ __global__ void moments_kernel(const S* __restrict__ pops, const Geometry g, boo
     rho = p->wall_rho; u[0] = u[1] = u[2] = R(0);
   } else if (kind == K_BOUNCE_BACK_VELOCITY) {
     rho = p->wall_rho; u[0] = p->wall_u[0]; u[1] = p->wall_u[1]; u[2] = p->wall_u[2];
-  } else if (is_interpolated(kind)) {
+  } else if (is_interpolated(kind) || kind == K_LOCAL_VELOCITY) {
     R f[Q];
     static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted); });
     bc_rho_u<L>(f, kind, p->bc_dir, p->bc_orient, p->bc_values + 4 * size_t(bc_index(p, x, y, z)), rho, u);
+  } else if (is_outer(kind)) {
+    // BulkDensity + FixedVelocityMomentumGeneric
+    R f[Q];
+    static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted); });
+    rho = compute_rho<L>(f);
+    const R* v = p->bc_values + 4 * size_t(bc_index(p, x, y, z));
+    u[0] = v[1]; u[1] = v[2]; u[2] = v[3];
   } else {
     rho = R(1); u[0] = u[1] = u[2] = R(0);
   }
@@ -730,28 +761,6 @@ OLB_DEV void logical_store(S* __restrict__ pops, const Geometry& g, int x, int y
   const uint32_t dst = cell_slot(g, wrap(x - L::c(I, 0), g.nx), wrap(y - L::c(I, 1), g.ny),
                                  wrap(z - L::c(I, 2), g.nz));
   Store<S, R>::template store<L, o>(pops + size_t(o) * g.stride + dst, v);
-}
-
-// equilibrium<DESCRIPTOR>::fromPiToFneq  src/dynamics/lbm.h:225-247
-template <class L, int I, class R>
-OLB_DEV R from_pi_to_fneq(const R (&pi)[6])
-{
-  R fneq = R(0);
-  static_for<0, 3>([&](auto a) {
-    static_for<a.value, 3>([&](auto b) {
-      constexpr int k = a.value * 3 - (a.value * (a.value - 1)) / 2 + (b.value - a.value);
-      R to_add = R(L::c(I, a) * L::c(I, b));
-      if constexpr (a.value == b.value) {
-        to_add -= R(1) / R(3);
-      } else {
-        to_add *= R(2);
-      }
-      to_add *= pi[k];
-      fneq += to_add;
-    });
-  });
-  fneq *= weight<L, R>(I) * R(3) * R(3) / R(2);
-  return fneq;
 }
 
 OLB_DEV void decode_cell(const Geometry& g, uint32_t n, int& x, int& y, int& z)
@@ -803,7 +812,46 @@ OLB_DEV void cell_velocity(const S* __restrict__ pops, const Geometry& g, bool s
   } else if (is_interpolated(kind)) {
     const R* bu = e->bc_u + 3 * size_t(bc_index(e, p[0], p[1], p[2]));
     u[0] = bu[0]; u[1] = bu[1]; u[2] = bu[2];
+  } else if (kind == K_LOCAL_VELOCITY || is_outer(kind)) {
+    // FixedVelocityMomentumGeneric: the VELOCITY field
+    const R* v = e->bc_values + 4 * size_t(bc_index(e, p[0], p[1], p[2]));
+    u[0] = v[1]; u[1] = v[2]; u[2] = v[3];
   }
+}
+
+// Cell::computeRho through the cell's dynamics on the current state:
+// BulkDensity (fluid, external edges and corners), velocityBMRho (flat velocity
+// boundaries), FixedDensity RHO (walls, pressure boundaries), 1 for NoDynamics
+// and for the reference's padding beyond a non-periodic face.
+template <int Q, class S, class R>
+OLB_DEV R cell_density(const S* __restrict__ pops, const Geometry& g, bool shifted,
+                       const uint8_t* __restrict__ ids, const DynDevice<R>* __restrict__ table, int periodic,
+                       int x, int y, int z)
+{
+  using L = Lattice<Q>;
+  int p[3] = {x, y, z};
+  const int ext[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (p[d] < 0 || p[d] >= ext[d]) {
+      if (!((periodic >> d) & 1)) return R(1);
+      p[d] = p[d] < 0 ? p[d] + ext[d] : p[d] - ext[d];
+    }
+  }
+  const uint32_t n = (uint32_t(p[0]) * uint32_t(g.ny) + uint32_t(p[1])) * uint32_t(g.nz) + uint32_t(p[2]);
+  const DynDevice<R>* e = table + ids[n];
+  const int kind = e->kind;
+  if (kind == K_BOUNCE_BACK || kind == K_BOUNCE_BACK_VELOCITY) return e->wall_rho;
+  if (kind == K_NONE) return R(1);
+  R f[Q];
+  static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, p[0], p[1], p[2], shifted); });
+  if (is_interpolated(kind) || kind == K_LOCAL_VELOCITY) {
+    R rho, u[3];
+    bc_rho_u<L>(f, kind, e->bc_dir, e->bc_orient, e->bc_values + 4 * size_t(bc_index(e, p[0], p[1], p[2])), rho,
+                u);
+    return rho;
+  }
+  return compute_rho<L>(f);
 }
 
 // pass 1: velocity of every interpolated cell (its momenta, post-stream state)
@@ -888,6 +936,146 @@ __global__ void plane_fd_kernel(S* __restrict__ pops, const Geometry g, bool shi
   });
 }
 
+// Collision of the boundary cells that carry values (interpolated, local
+// velocity, external edges and corners), in place, ahead of the step kernel.
+// Each cell's populations are read where the step kernel will read them
+// (the current AA parity) and written back there, so the step kernel, which
+// passes these cells through, streams the collided values.  Keeping the
+// boundary collisions out of the step kernel leaves its register allocation
+// to the bulk collision: inlined, they raised the register demand of every
+// cell and the masked kernels spilled.  Statistics of the boundary cells go
+// to the partials after the step kernel's blocks.
+template <int Q, class S, class R, int KIND, bool STATS>
+__global__ void boundary_collide_kernel(S* __restrict__ pops, const Geometry g, bool shifted,
+                                        const uint8_t* __restrict__ ids, const DynDevice<R>* __restrict__ table,
+                                        const uint32_t* __restrict__ cells, uint32_t count,
+                                        StatPartial* __restrict__ partials)
+{
+  using L = Lattice<Q>;
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  double s_rho = 0., s_usqr = 0., s_max = 0.;
+  unsigned long long s_n = 0, s_nf = 0;
+  if (k < count) {
+    const uint32_t n = cells[k];
+    int x, y, z;
+    decode_cell(g, n, x, y, z);
+    const DynDevice<R>* e = table + ids[n];
+    R f[Q];
+    static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted); });
+    R st_rho = R(0), st_usqr = R(0);
+    collide_boundary<L, KIND>(f, e->kind, e, x, y, z, st_rho, st_usqr);
+    static_for<0, Q>([&](auto i) { logical_store<Q, S, R, i.value>(pops, g, x, y, z, shifted, f[i]); });
+    if constexpr (STATS) {
+      const double r = double(st_rho), u2 = double(st_usqr);
+      if (isfinite(r) && isfinite(u2)) {
+        s_rho = r; s_usqr = u2; s_max = u2; s_n = 1;
+      } else {
+        s_nf = 1;
+      }
+    }
+  }
+  if constexpr (STATS) {
+    block_stats(s_rho, s_usqr, s_max, s_n, s_nf, partials);
+  }
+}
+
+// OuterVelocityEdgeProcessor3D<plane,normal1,normal2>::apply (pass 3) and
+// OuterVelocityCornerProcessor3D<xN,yN,zN>::apply (pass 4),
+// src/boundary/boundaryPostProcessors3D.hh:164-292: the density extrapolated
+// from the cells inward along the normal(s), velocity gradients one-sided
+// across the boundary and central along an edge, the cell rebuilt as
+// feq(rho, VELOCITY) + fneq(Pi).  The corner pass runs after the edge pass
+// (priority 1 after 0): a corner's density reads the edge cells it ends.
+template <int Q, class S, class R, bool CORNER>
+__global__ void outer_velocity_kernel(S* __restrict__ pops, const Geometry g, bool shifted,
+                                      const uint8_t* __restrict__ ids, const DynDevice<R>* __restrict__ table,
+                                      int periodic, const uint32_t* __restrict__ cells, uint32_t count)
+{
+  using L = Lattice<Q>;
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const uint32_t n = cells[k];
+  int x, y, z;
+  decode_cell(g, n, x, y, z);
+  const DynDevice<R>* e = table + ids[n];
+  const int nrm[3] = {e->nrm[0], e->nrm[1], e->nrm[2]};
+  const R* v = e->bc_values + 4 * size_t(bc_index(e, x, y, z));
+  const R u[3] = {v[1], v[2], v[3]};
+  R rho;
+  R grad[3][3];  // grad[d][c]: derivative along axis d of velocity component c
+  if constexpr (!CORNER) {
+    const int plane = nrm[0] == 0 ? 0 : (nrm[1] == 0 ? 1 : 2);
+    const int d1 = plane == 2 ? 0 : plane + 1, d2 = plane == 0 ? 2 : (plane == 1 ? 0 : 1);
+    // getNeighborRho(step1, step2): offset -normal1 step1 along d1, -normal2 step2 along d2
+    R r[4];  // rho10, rho01, rho20, rho02
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const int s1 = m == 0 ? 1 : (m == 2 ? 2 : 0), s2 = m == 1 ? 1 : (m == 3 ? 2 : 0);
+      int o[3] = {0, 0, 0};
+      o[d1] = -nrm[d1] * s1;
+      o[d2] = -nrm[d2] * s2;
+      r[m] = cell_density<Q, S, R>(pops, g, shifted, ids, table, periodic, x + o[0], y + o[1], z + o[2]);
+    }
+    rho = R(2) / R(3) * (r[1] + r[0]) - R(1) / R(6) * (r[3] + r[2]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int ex = d == 0, ey = d == 1, ez = d == 2;
+      if (d == plane) {
+        R up[3], um[3];
+        cell_velocity<Q, S, R>(pops, g, shifted, ids, table, periodic, x + ex, y + ey, z + ez, up);
+        cell_velocity<Q, S, R>(pops, g, shifted, ids, table, periodic, x - ex, y - ey, z - ez, um);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) grad[d][c] = (up[c] - um[c]) / R(2);
+      } else {
+        const int s = -nrm[d];
+        R u1[3], u2[3];
+        cell_velocity<Q, S, R>(pops, g, shifted, ids, table, periodic, x + s * ex, y + s * ey, z + s * ez, u1);
+        cell_velocity<Q, S, R>(pops, g, shifted, ids, table, periodic, x + 2 * s * ex, y + 2 * s * ey,
+                               z + 2 * s * ez, u2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          grad[d][c] = R(-nrm[d]) * ((-R(3) * u[c] + R(4) * u1[c] - R(1) * u2[c]) / R(2));
+        }
+      }
+    }
+  } else {
+    R r[6];  // rho100, rho010, rho001, rho200, rho020, rho002
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      int o[3] = {0, 0, 0};
+      o[m % 3] = -(m / 3 + 1) * nrm[m % 3];
+      r[m] = cell_density<Q, S, R>(pops, g, shifted, ids, table, periodic, x + o[0], y + o[1], z + o[2]);
+    }
+    rho = R(4) / R(9) * (r[2] + r[1] + r[0]) - R(1) / R(9) * (r[5] + r[4] + r[3]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int ex = d == 0, ey = d == 1, ez = d == 2;
+      const int s = -nrm[d];
+      R u1[3], u2[3];
+      cell_velocity<Q, S, R>(pops, g, shifted, ids, table, periodic, x + s * ex, y + s * ey, z + s * ez, u1);
+      cell_velocity<Q, S, R>(pops, g, shifted, ids, table, periodic, x + 2 * s * ex, y + 2 * s * ey,
+                             z + 2 * s * ez, u2);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        grad[d][c] = R(-nrm[d]) * ((-R(3) * u[c] + R(4) * u1[c] - R(1) * u2[c]) / R(2));
+      }
+    }
+  }
+  const R s_to_pi = -rho / R(3) / e->omega;
+  R pi[6];
+  pi[0] = R(2) * grad[0][0] * s_to_pi;
+  pi[3] = R(2) * grad[1][1] * s_to_pi;
+  pi[5] = R(2) * grad[2][2] * s_to_pi;
+  pi[1] = (grad[0][1] + grad[1][0]) * s_to_pi;
+  pi[2] = (grad[0][2] + grad[2][0]) * s_to_pi;
+  pi[4] = (grad[1][2] + grad[2][1]) * s_to_pi;
+  const R usqr = norm_sqr(u);
+  static_for<0, Q>([&](auto i) {
+    const R val = feq2<L, i.value>(rho, u, usqr) + from_pi_to_fneq<L, i.value>(pi);
+    logical_store<Q, S, R, i.value>(pops, g, x, y, z, shifted, val);
+  });
+}
+
 // ---------------------------------------------------------------------------
 // host-side launch entry points (explicitly instantiated per lattice/storage)
 
@@ -918,10 +1106,20 @@ template <int Q, class S, class R>
 cudaError_t launch_moments(const void* pops, const Geometry& g, bool shifted, const uint8_t* ids,
                            const void* table, void* rho, void* u, cudaStream_t stream);
 
-// both PostStream passes over `count` interpolated cells
+// the boundary pre-pass over `count` cells; partials == nullptr: no statistics
+template <int Q, class S, class R>
+cudaError_t launch_boundary_collide(void* pops, const Geometry& g, bool shifted, const uint8_t* ids,
+                                    const void* table, int kind, const uint32_t* cells, uint32_t count,
+                                    StatPartial* partials, cudaStream_t stream);
+constexpr int kBoundaryThreads = 128;
+
+// the PostStream passes: cells[0, n_flat) are the interpolated flat cells
+// (velocity pass, then PlaneFd), the next n_edge the external edge cells,
+// the last n_corner the external corner cells
 template <int Q, class S, class R>
 cudaError_t launch_boundary(void* pops, const Geometry& g, bool shifted, const uint8_t* ids, const void* table,
-                            int periodic, const uint32_t* cells, uint32_t count, cudaStream_t stream);
+                            int periodic, const uint32_t* cells, uint32_t n_flat, uint32_t n_edge,
+                            uint32_t n_corner, cudaStream_t stream);
 
 inline dim3 step_grid(const Geometry& g, int bz, int by, int cells_per_thread)
 {

@@ -112,20 +112,65 @@ cudaError_t launch_moments(const void* pops, const Geometry& g, bool shifted, co
 }
 
 template <int Q, class S, class R>
-cudaError_t launch_boundary(void* pops, const Geometry& g, bool shifted, const uint8_t* ids, const void* table,
-                            int periodic, const uint32_t* cells, uint32_t count, cudaStream_t stream)
+cudaError_t launch_boundary_collide(void* pops, const Geometry& g, bool shifted, const uint8_t* ids,
+                                    const void* table, int kind, const uint32_t* cells, uint32_t count,
+                                    StatPartial* partials, cudaStream_t stream)
 {
   if (count == 0) return cudaSuccess;
-  const int threads = 128;
-  const unsigned blocks = (count + threads - 1) / threads;
+  const unsigned blocks = (count + kBoundaryThreads - 1) / kBoundaryThreads;
+  S* p = static_cast<S*>(pops);
   const auto* t = static_cast<const DynDevice<R>*>(table);
-  bc_velocity_kernel<Q, S, R><<<blocks, threads, 0, stream>>>(static_cast<const S*>(pops), g, shifted, ids, t,
-                                                              cells, count);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  plane_fd_kernel<Q, S, R><<<blocks, threads, 0, stream>>>(static_cast<S*>(pops), g, shifted, ids, t, periodic,
-                                                           cells, count);
+#define OLB_BC_LAUNCH(K)                                                                             \
+  do {                                                                                               \
+    if (partials)                                                                                    \
+      boundary_collide_kernel<Q, S, R, K, true><<<blocks, kBoundaryThreads, 0, stream>>>(            \
+        p, g, shifted, ids, t, cells, count, partials);                                              \
+    else                                                                                             \
+      boundary_collide_kernel<Q, S, R, K, false><<<blocks, kBoundaryThreads, 0, stream>>>(           \
+        p, g, shifted, ids, t, cells, count, partials);                                              \
+  } while (0)
+  switch (kind) {
+  case K_TRT: OLB_BC_LAUNCH(K_TRT); break;
+  case K_SMAGORINSKY: OLB_BC_LAUNCH(K_SMAGORINSKY); break;
+  default: OLB_BC_LAUNCH(K_BGK); break;
+  }
+#undef OLB_BC_LAUNCH
   return cudaGetLastError();
+}
+
+template <int Q, class S, class R>
+cudaError_t launch_boundary(void* pops, const Geometry& g, bool shifted, const uint8_t* ids, const void* table,
+                            int periodic, const uint32_t* cells, uint32_t n_flat, uint32_t n_edge,
+                            uint32_t n_corner, cudaStream_t stream)
+{
+  const int threads = 128;
+  const auto* t = static_cast<const DynDevice<R>*>(table);
+  cudaError_t e = cudaSuccess;
+  if (n_flat) {
+    const unsigned blocks = (n_flat + threads - 1) / threads;
+    bc_velocity_kernel<Q, S, R><<<blocks, threads, 0, stream>>>(static_cast<const S*>(pops), g, shifted, ids, t,
+                                                                cells, n_flat);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    plane_fd_kernel<Q, S, R><<<blocks, threads, 0, stream>>>(static_cast<S*>(pops), g, shifted, ids, t, periodic,
+                                                             cells, n_flat);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (n_edge) {
+    const unsigned blocks = (n_edge + threads - 1) / threads;
+    outer_velocity_kernel<Q, S, R, false><<<blocks, threads, 0, stream>>>(
+      static_cast<S*>(pops), g, shifted, ids, t, periodic, cells + n_flat, n_edge);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (n_corner) {
+    const unsigned blocks = (n_corner + threads - 1) / threads;
+    outer_velocity_kernel<Q, S, R, true><<<blocks, threads, 0, stream>>>(
+      static_cast<S*>(pops), g, shifted, ids, t, periodic, cells + n_flat + n_edge, n_corner);
+    e = cudaGetLastError();
+  }
+  return e;
 }
 
 } // namespace olb_b200
@@ -139,7 +184,10 @@ cudaError_t launch_boundary(void* pops, const Geometry& g, bool shifted, const u
                                                cudaStream_t);                                      \
   template cudaError_t launch_moments<Q, S, R>(const void*, const Geometry&, bool, const uint8_t*, \
                                                const void*, void*, void*, cudaStream_t);           \
+  template cudaError_t launch_boundary_collide<Q, S, R>(void*, const Geometry&, bool, const uint8_t*, \
+                                                        const void*, int, const uint32_t*, uint32_t, \
+                                                        StatPartial*, cudaStream_t);               \
   template cudaError_t launch_boundary<Q, S, R>(void*, const Geometry&, bool, const uint8_t*,      \
                                                 const void*, int, const uint32_t*, uint32_t,       \
-                                                cudaStream_t);                                     \
+                                                uint32_t, uint32_t, cudaStream_t);                 \
   }

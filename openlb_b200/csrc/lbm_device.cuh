@@ -109,10 +109,15 @@ OLB_HD constexpr float storage_scale(int i)
 enum DynKind : int32_t {
   K_NONE = 0, K_BGK = 1, K_TRT = 2, K_SMAGORINSKY = 3, K_BOUNCE_BACK = 4,
   K_BOUNCE_BACK_VELOCITY = 5, K_FORCED_BGK = 6, K_FORCED_TRT = 7,
-  K_INTERP_VELOCITY = 8, K_INTERP_PRESSURE = 9
+  K_INTERP_VELOCITY = 8, K_INTERP_PRESSURE = 9,
+  K_LOCAL_VELOCITY = 10, K_VELOCITY_EDGE = 11, K_VELOCITY_CORNER = 12
 };
 
 OLB_HD bool is_interpolated(int kind) { return kind == K_INTERP_VELOCITY || kind == K_INTERP_PRESSURE; }
+// external edges and corners of velocity boundaries (OuterVelocity*Processor3D)
+OLB_HD bool is_outer(int kind) { return kind == K_VELOCITY_EDGE || kind == K_VELOCITY_CORNER; }
+// boundary cells whose values (RHO, VELOCITY) live in their entry's value box
+OLB_HD bool has_values(int kind) { return is_interpolated(kind) || kind == K_LOCAL_VELOCITY || is_outer(kind); }
 
 template <class R>
 struct DynDevice {
@@ -131,6 +136,8 @@ struct DynDevice {
   int32_t bc_dir;     // axis of the outward normal
   int32_t bc_orient;  // its sign, -1 or +1
   int32_t box[6];     // x0, y0, z0 and extents of the bounding box of the entry's cells
+  int32_t nrm[3];     // edges and corners: the discrete normal
+  int32_t nrm_pad;
   const R* bc_values; // per box cell: RHO, VELOCITY x, y, z (4 values)
   R* bc_u;            // per box cell: velocity of the post-stream state (3 values)
 };
@@ -296,6 +303,26 @@ OLB_DEV void relax_trt_reference(R (&f)[L::q], R rho, const R (&u)[3], R omega, 
   static_for<0, L::q>([&](auto i) { f[i] = out[i]; });
 }
 
+// The equilibrium's momentum coefficient 3 w_i (with inv_cs2 = 3) applied to
+// x = rho (c_i . u) (times omega in the scaled form), with 3 w_i held as an
+// unevaluated sum hi + lo of two R values.  hi alone is biased: in FP32
+// fl(1/6) = fl(3/18) and fl(1/12) = fl(3/36) both exceed the exact value by
+// the same 3.0e-8 relative, so the equilibrium's momentum sum_i hi_i c_i c_i
+// rho u = (1 + 3.0e-8) rho u, and each relaxation adds omega times that bias
+// to the fluid's momentum: a velocity drift that grows linearly with the step
+// count (3e-4 of the velocity after 5000 steps of the 256^3 Taylor-Green
+// vortex).  x hi + x lo, fused, keeps the coefficient to within rounding of
+// x; the reference's form rho t (1 + 3 c.u + ...) carries the smaller bias
+// of fl(1/18) (7.5e-9).  In FP64 lo is zero.
+template <class L, class R, int I>
+OLB_DEV R momentum_term(R x)
+{
+  constexpr double exact = 3.0 * double(L::wnum(I)) / double(L::wden(I));
+  constexpr R hi = R(exact);
+  constexpr R lo = R(exact - double(hi));
+  return fma(x, hi, x * lo);
+}
+
 // The same two collisions evaluated over opposite pairs.  For c_o = -c_i the
 // second-order equilibria share their even part:
 //   feq_i = A + B,  feq_o = A - B,
@@ -321,7 +348,7 @@ OLB_DEV void relax_bgk_paired(R (&f)[L::q], R rho, R delta, const R (&u)[3], R o
     const R cu = c_dot<L, i.value>(u);
     const R ev = R(4.5) * cu * cu + e0;
     const R a = t * (delta + rho * ev);
-    const R b = (rho * (R(3) * t)) * cu;
+    const R b = momentum_term<L, R, i.value>(rho * cu);
     const R fi = keep * f[i] + omega * (a + b);
     const R fo = keep * f[o] + omega * (a - b);
     f[i] = fi;
@@ -344,7 +371,7 @@ OLB_DEV void relax_trt_paired(R (&f)[L::q], R rho, R delta, const R (&u)[3], R o
     const R cu = c_dot<L, i.value>(u);
     const R ev = R(4.5) * cu * cu + e0;
     const R a = t * (delta + rho * ev);                 // symmetric part of feq
-    const R b = (rho * (R(3) * t)) * cu;                // antisymmetric part
+    const R b = momentum_term<L, R, i.value>(rho * cu);   // antisymmetric part
     const R dp = omega * (R(0.5) * (f[i] + f[o]) - a);
     const R dm = omega_minus * (R(0.5) * (f[i] - f[o]) - b);
     const R fi = f[i] - dp - dm;
@@ -593,7 +620,7 @@ OLB_DEV void bc_rho_u(const R (&f)[L::q], int kind, int dir, int orient, const R
   u[1] = v[2];
   u[2] = v[3];
   const R so = R(orient);
-  if (kind == K_INTERP_VELOCITY) {
+  if (kind != K_INTERP_PRESSURE) {
     const R ud = dir == 0 ? u[0] : (dir == 1 ? u[1] : u[2]);
     rho = (R(2) * normal + on_wall + R(1)) / (R(1) + so * ud);
   } else {
@@ -631,6 +658,136 @@ OLB_DEV void collide_interpolated(R (&f)[L::q], int kind, const DynDevice<R>* __
   }
   st_rho = rho;
   st_usqr = norm_sqr(u);
+}
+
+// equilibrium<DESCRIPTOR>::fromPiToFneq  src/dynamics/lbm.h:225-247
+template <class L, int I, class R>
+OLB_DEV R from_pi_to_fneq(const R (&pi)[6])
+{
+  R fneq = R(0);
+  static_for<0, 3>([&](auto a) {
+    static_for<a.value, 3>([&](auto b) {
+      constexpr int k = a.value * 3 - (a.value * (a.value - 1)) / 2 + (b.value - a.value);
+      R to_add = R(L::c(I, a) * L::c(I, b));
+      if constexpr (a.value == b.value) {
+        to_add -= R(1) / R(3);
+      } else {
+        to_add *= R(2);
+      }
+      to_add *= pi[k];
+      fneq += to_add;
+    });
+  });
+  fneq *= weight<L, R>(I) * R(3) * R(3) / R(2);
+  return fneq;
+}
+
+// BoundaryHelpers<T,DESCRIPTOR,direction,orientation>::computeStress
+// (src/boundary/helper.h:31-80), the stress of momenta::RegularizedBoundaryStress
+// (src/dynamics/momenta/elements.h:1667-1673): non-equilibrium parts of the
+// populations in the wall plane (c_i[dir] == 0; the rest population counts as
+// zero) and, doubled, of those along the outward normal, each set in ascending
+// population order.
+template <class L, class R>
+OLB_DEV void boundary_stress(const R (&f)[L::q], int dir, int orient, R rho, const R (&u)[3], R (&pi)[6])
+{
+  const R usqr = norm_sqr(u);
+  R fneq[L::q];
+  static_for<0, L::q>([&](auto i) {
+    constexpr int c0 = L::c(i, 0), c1 = L::c(i, 1), c2 = L::c(i, 2);
+    const int cd = dir == 0 ? c0 : (dir == 1 ? c1 : c2);
+    fneq[i] = R(0);
+    if ((cd == 0 && i.value != 0) || cd == orient) {
+      fneq[i] = f[i] - feq2<L, i.value>(rho, u, usqr);
+    }
+  });
+  static_for<0, 3>([&](auto a) {
+    static_for<a.value, 3>([&](auto b) {
+      constexpr int k = a.value * 3 - (a.value * (a.value - 1)) / 2 + (b.value - a.value);
+      R sum = R(0);
+      static_for<0, L::q>([&](auto i) {
+        constexpr int cab = L::c(i, a) * L::c(i, b);
+        const int cd = dir == 0 ? L::c(i, 0) : (dir == 1 ? L::c(i, 1) : L::c(i, 2));
+        if (cd == 0) sum += R(cab) * fneq[i];
+      });
+      static_for<0, L::q>([&](auto i) {
+        constexpr int cab = L::c(i, a) * L::c(i, b);
+        const int cd = dir == 0 ? L::c(i, 0) : (dir == 1 ? L::c(i, 1) : L::c(i, 2));
+        if (cd == orient) sum += R(2 * cab) * fneq[i];
+      });
+      pi[k] = sum;
+    });
+  });
+}
+
+// CombinedRLBdynamics<MIXIN, RegularizedVelocityBoundaryTuple<dir,orient>>::collide
+// (src/dynamics/dynamics.h:419-430): momenta rho = velocityBMRho, u = VELOCITY,
+// pi = the regularised boundary stress; the populations are rebuilt as
+// feq + fneq(pi), then the mixin collides with the same momenta evaluated
+// again on the rebuilt cell.
+template <class L, int KIND, class R>
+OLB_DEV void collide_local_velocity(R (&f)[L::q], const DynDevice<R>* __restrict__ e, int x, int y, int z,
+                                    R& st_rho, R& st_usqr)
+{
+  const R* __restrict__ v = e->bc_values + 4 * size_t(bc_index(e, x, y, z));
+  const int dir = e->bc_dir, orient = e->bc_orient;
+  R rho, u[3], pi[6];
+  bc_rho_u<L>(f, K_LOCAL_VELOCITY, dir, orient, v, rho, u);
+  boundary_stress<L>(f, dir, orient, rho, u, pi);
+  {
+    const R usqr = norm_sqr(u);
+    static_for<0, L::q>([&](auto i) { f[i] = feq2<L, i.value>(rho, u, usqr) + from_pi_to_fneq<L, i.value>(pi); });
+  }
+  bc_rho_u<L>(f, K_LOCAL_VELOCITY, dir, orient, v, rho, u);
+  const R delta = rho - R(1);
+  if constexpr (KIND == K_TRT) {
+    relax_trt<L>(f, rho, delta, u, e->omega, e->omega_minus);
+  } else {
+    relax_bgk<L>(f, rho, delta, u, e->omega);
+  }
+  st_rho = rho;
+  st_usqr = norm_sqr(u);
+}
+
+// MIXIN::exchange_momenta<FixedVelocityBoundaryTuple> (src/dynamics/momenta/
+// aliases.h:188-193) on external edges and corners: BulkDensity and
+// u = VELOCITY; the mixin collision on those momenta.
+template <class L, int KIND, class R>
+OLB_DEV void collide_fixed_velocity(R (&f)[L::q], const DynDevice<R>* __restrict__ e, int x, int y, int z,
+                                    R& st_rho, R& st_usqr)
+{
+  const R* __restrict__ v = e->bc_values + 4 * size_t(bc_index(e, x, y, z));
+  R delta = f[0];
+  static_for<1, L::q>([&](auto i) { delta += f[i]; });
+  const R rho = delta + R(1);
+  const R u[3] = {v[1], v[2], v[3]};
+  if constexpr (KIND == K_TRT) {
+    relax_trt<L>(f, rho, delta, u, e->omega, e->omega_minus);
+  } else if constexpr (KIND == K_SMAGORINSKY) {
+    const R w = smagorinsky_omega<L>(f, rho, delta, u, e->smago_pre, e->tau_mol);
+    relax_bgk<L>(f, rho, delta, u, w);
+  } else {
+    relax_bgk<L>(f, rho, delta, u, e->omega);
+  }
+  st_rho = rho;
+  st_usqr = norm_sqr(u);
+}
+
+// collision of a boundary cell that carries values, by its runtime kind
+// (run by boundary_collide_kernel, ahead of the step kernel)
+template <class L, int KIND, class R>
+OLB_DEV void collide_boundary(R (&f)[L::q], int kind, const DynDevice<R>* __restrict__ e, int x, int y, int z,
+                              R& st_rho, R& st_usqr)
+{
+  if (is_interpolated(kind)) {
+    collide_interpolated<L, KIND>(f, kind, e, x, y, z, st_rho, st_usqr);
+  } else if (kind == K_LOCAL_VELOCITY) {
+    if constexpr (KIND == K_BGK || KIND == K_TRT) {
+      collide_local_velocity<L, KIND>(f, e, x, y, z, st_rho, st_usqr);
+    }
+  } else {
+    collide_fixed_velocity<L, KIND>(f, e, x, y, z, st_rho, st_usqr);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -715,7 +872,9 @@ OLB_DEV void relax_bgk_scaled(float (&g)[L::q], float rho, float delta, const fl
     const float cu = c_dot<L, i.value>(u);
     const float ev = 4.5f * cu * cu + e0;
     const float a = wt * (delta + rho * ev);
-    const float b = (rho * (3.f * wt)) * cu;
+    // 3 s_i w_i omega (rho c.u): s_i is a power of two, so the scaled
+    // coefficient has the same hi + lo split as 3 w_i
+    const float b = storage_scale<L>(i) * momentum_term<L, float, i.value>(omega * (rho * cu));
     g[i] = (keep * g[i] + a) + b;
     g[o] = (keep * g[o] + a) - b;
   });
@@ -737,7 +896,7 @@ OLB_DEV void relax_trt_scaled(float (&g)[L::q], float rho, float delta, const fl
     const float cu = c_dot<L, i.value>(u);
     const float ev = 4.5f * cu * cu + e0;
     const float a = T * (delta + rho * ev);
-    const float b = (rho * (3.f * T)) * cu;
+    const float b = storage_scale<L>(i) * momentum_term<L, float, i.value>(rho * cu);
     const float dp = omega * (0.5f * (g[i] + g[o]) - a);
     const float dm = omega_minus * (0.5f * (g[i] - g[o]) - b);
     const float gi = g[i] - dp - dm;

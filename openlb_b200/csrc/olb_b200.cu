@@ -30,9 +30,13 @@ namespace olb_b200 {
   extern template cudaError_t launch_moments<Q, S, R>(const void*, const Geometry&, bool,          \
                                                       const uint8_t*, const void*, void*, void*,   \
                                                       cudaStream_t);                               \
+  extern template cudaError_t launch_boundary_collide<Q, S, R>(void*, const Geometry&, bool,       \
+                                                               const uint8_t*, const void*, int,   \
+                                                               const uint32_t*, uint32_t,          \
+                                                               StatPartial*, cudaStream_t);        \
   extern template cudaError_t launch_boundary<Q, S, R>(void*, const Geometry&, bool, const uint8_t*, \
                                                        const void*, int, const uint32_t*, uint32_t, \
-                                                       cudaStream_t);
+                                                       uint32_t, uint32_t, cudaStream_t);
 OLB_B200_EXTERN(19, float, float)
 OLB_B200_EXTERN(19, double, double)
 OLB_B200_EXTERN(19, __half, float)
@@ -273,8 +277,9 @@ struct olb_b200_lattice {
   std::vector<BcBox> bc_box;        // per table entry
   std::vector<uint8_t> ids_host;    // per cell (kept while boundary entries exist)
   std::vector<double> bc_host;      // 4 values per slot, host copy
-  uint32_t* bc_cells = nullptr;     // device: cell index of every boundary cell
-  uint32_t n_bc = 0;
+  uint32_t* bc_cells = nullptr;     // device: flat interpolated, then edge, then corner cells
+  uint32_t n_bc = 0;                // cells in bc_cells
+  uint32_t n_bc_flat = 0, n_bc_edge = 0, n_bc_corner = 0;  // PostStream segments; local faces follow
   void* bc_values = nullptr;        // device: 4 R per slot
   void* bc_u = nullptr;             // device: 3 R per slot
   size_t bc_slots = 0;
@@ -341,10 +346,61 @@ cudaError_t dispatch(const olb_b200_lattice* L, F&& f)
 
 olb_b200_status ensure_partial_count(olb_b200_lattice* L, size_t need);
 
-olb_b200_status ensure_partials(olb_b200_lattice* L)
+// blocks of the boundary collision pre-pass (their statistics follow the step kernel's)
+size_t boundary_blocks(const olb_b200_lattice* L)
+{
+  return (size_t(L->n_bc) + kBoundaryThreads - 1) / kBoundaryThreads;
+}
+
+size_t step_blocks(const olb_b200_lattice* L)
 {
   const dim3 grid = step_grid(L->g, L->block_z, L->block_y, cells_per_thread(L));
-  return ensure_partial_count(L, size_t(grid.x) * grid.y * grid.z);
+  return size_t(grid.x) * grid.y * grid.z;
+}
+
+// The bulk box of a masked lattice: a box all of whose cells use the bulk
+// entry, so the step kernel loads no dynamics id for them.  The box starts as
+// the whole lattice and loses any face layer that holds another entry until
+// no face does (for a lattice with walls on its faces, such as the lid-driven
+// cavity, that is the interior); if the box's interior still holds another
+// entry (obstacles inside), no box is used.
+void compute_bulk_box(olb_b200_lattice* L, const uint8_t* ids, int bulk_entry)
+{
+  Geometry& g = L->g;
+  for (int d = 0; d < 3; ++d) g.bulk_lo[d] = g.bulk_hi[d] = 0;
+  if (!ids || bulk_entry < 0) return;
+  const int n[3] = {L->desc.nx, L->desc.ny, L->desc.nz};
+  auto id_at = [&](int x, int y, int z) { return int(ids[(size_t(x) * n[1] + y) * n[2] + z]); };
+  int lo[3] = {0, 0, 0}, hi[3] = {n[0], n[1], n[2]};
+  auto face_clean = [&](int axis, int layer) {
+    int a[3], b[3];
+    for (int d = 0; d < 3; ++d) { a[d] = lo[d]; b[d] = hi[d]; }
+    a[axis] = layer;
+    b[axis] = layer + 1;
+    for (int x = a[0]; x < b[0]; ++x)
+      for (int y = a[1]; y < b[1]; ++y)
+        for (int z = a[2]; z < b[2]; ++z)
+          if (id_at(x, y, z) != bulk_entry) return false;
+    return true;
+  };
+  for (bool changed = true; changed;) {
+    changed = false;
+    for (int d = 0; d < 3 && lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2]; ++d) {
+      if (!face_clean(d, lo[d])) { ++lo[d]; changed = true; }
+      if (lo[d] < hi[d] && !face_clean(d, hi[d] - 1)) { --hi[d]; changed = true; }
+    }
+    if (!(lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2])) return;
+  }
+  for (int x = lo[0]; x < hi[0]; ++x)
+    for (int y = lo[1]; y < hi[1]; ++y)
+      for (int z = lo[2]; z < hi[2]; ++z)
+        if (id_at(x, y, z) != bulk_entry) return;
+  for (int d = 0; d < 3; ++d) { g.bulk_lo[d] = lo[d]; g.bulk_hi[d] = hi[d]; }
+}
+
+olb_b200_status ensure_partials(olb_b200_lattice* L)
+{
+  return ensure_partial_count(L, step_blocks(L) + boundary_blocks(L));
 }
 
 olb_b200_status ensure_partial_count(olb_b200_lattice* L, size_t need)
@@ -373,7 +429,8 @@ olb_b200_status post_stream(olb_b200_lattice* L)
   if (L->n_bc == 0) return OLB_B200_OK;
   cudaError_t e = dispatch(L, [&](auto qc, auto s_, auto r_) {
     return launch_boundary<decltype(qc)::value, decltype(s_), decltype(r_)>(
-      L->pops, L->g, L->parity == 1, L->ids, L->table, periodic_mask(L), L->bc_cells, L->n_bc, L->stream);
+      L->pops, L->g, L->parity == 1, L->ids, L->table, periodic_mask(L), L->bc_cells, L->n_bc_flat,
+      L->n_bc_edge, L->n_bc_corner, L->stream);
   });
   if (e != cudaSuccess) return cuda_fail(e, "boundary post-processing kernels");
   return OLB_B200_OK;
@@ -410,7 +467,17 @@ olb_b200_status enqueue_steps(olb_b200_lattice* L, int steps, bool stats_last)
     a.variant = L->variant;
     a.stream = L->stream;
     const bool odd = L->parity == 1;
-    cudaError_t e = dispatch(L, [&](auto qc, auto s_, auto r_) {
+    cudaError_t e = cudaSuccess;
+    if (L->n_bc) {
+      // collision of the boundary cells in place, ahead of the step kernel
+      StatPartial* bp = stats ? L->partials + step_blocks(L) : nullptr;
+      e = dispatch(L, [&](auto qc, auto s_, auto r_) {
+        return launch_boundary_collide<decltype(qc)::value, decltype(s_), decltype(r_)>(
+          L->pops, L->g, odd, L->ids, L->table, L->bulk_kind, L->bc_cells, L->n_bc, bp, L->stream);
+      });
+      if (e != cudaSuccess) return cuda_fail(e, "boundary collision launch");
+    }
+    e = dispatch(L, [&](auto qc, auto s_, auto r_) {
       using S = decltype(s_);
       using R = decltype(r_);
       return launch_step<decltype(qc)::value, S, R>(a, L->bulk_kind, odd, L->masked, stats);
@@ -443,6 +510,7 @@ olb_b200_status setup_boundaries(olb_b200_lattice* L, const uint8_t* ids, const 
   L->device_bytes -= L->bc_bytes;
   L->bc_bytes = 0;
   L->n_bc = 0;
+  L->n_bc_flat = L->n_bc_edge = L->n_bc_corner = 0;
   L->bc_slots = 0;
   L->bc_box.assign(size_t(n_entries), olb_b200_lattice::BcBox{{0, 0, 0, 0, 0, 0}, 0});
   L->bc_host.clear();
@@ -450,14 +518,21 @@ olb_b200_status setup_boundaries(olb_b200_lattice* L, const uint8_t* ids, const 
   if (!any) return OLB_B200_OK;
   const int nx = L->desc.nx, ny = L->desc.ny, nz = L->desc.nz;
   std::vector<int> lo(size_t(n_entries) * 3, INT32_MAX), hi(size_t(n_entries) * 3, -1);
-  std::vector<uint32_t> cells;
+  // PostStream order: flat interpolated cells (velocity pass, PlaneFd), then
+  // external edges, then external corners; local velocity faces need no
+  // PostStream pass and come last (the boundary collision pre-pass takes all)
+  std::vector<uint32_t> flat, edges, corners, local;
   for (int x = 0; x < nx; ++x) {
     for (int y = 0; y < ny; ++y) {
       for (int z = 0; z < nz; ++z) {
         const size_t c = (size_t(x) * ny + y) * nz + z;
         const int k = ids[c];
-        if (!is_interpolated(table[k].kind)) continue;
-        cells.push_back(uint32_t(c));
+        const int kind = table[k].kind;
+        if (!has_values(kind)) continue;
+        if (is_interpolated(kind)) flat.push_back(uint32_t(c));
+        else if (kind == K_VELOCITY_EDGE) edges.push_back(uint32_t(c));
+        else if (kind == K_VELOCITY_CORNER) corners.push_back(uint32_t(c));
+        else local.push_back(uint32_t(c));
         const int p[3] = {x, y, z};
         for (int d = 0; d < 3; ++d) {
           lo[3 * k + d] = std::min(lo[3 * k + d], p[d]);
@@ -477,19 +552,27 @@ olb_b200_status setup_boundaries(olb_b200_lattice* L, const uint8_t* ids, const 
     b.slot0 = slots;
     slots += size_t(b.box[3]) * b.box[4] * b.box[5];
   }
-  if (cells.empty()) return OLB_B200_OK;
+  if (slots == 0) return OLB_B200_OK;
+  std::vector<uint32_t> cells(flat);
+  cells.insert(cells.end(), edges.begin(), edges.end());
+  cells.insert(cells.end(), corners.begin(), corners.end());
+  cells.insert(cells.end(), local.begin(), local.end());
+  L->n_bc_flat = uint32_t(flat.size());
+  L->n_bc_edge = uint32_t(edges.size());
+  L->n_bc_corner = uint32_t(corners.size());
   L->ids_host.assign(ids, ids + L->cells);
   L->bc_slots = slots;
   L->bc_host.assign(4 * slots, 0.0);
   for (size_t k = 0; k < slots; ++k) L->bc_host[4 * k] = 1.0;
   L->n_bc = uint32_t(cells.size());
-  OLB_CUDA(cudaMalloc(&L->bc_cells, cells.size() * sizeof(uint32_t)));
+  OLB_CUDA(cudaMalloc(&L->bc_cells, std::max<size_t>(cells.size(), 1) * sizeof(uint32_t)));
   OLB_CUDA(cudaMalloc(&L->bc_values, 4 * slots * L->real));
   OLB_CUDA(cudaMalloc(&L->bc_u, 3 * slots * L->real));
   OLB_CUDA(cudaMemset(L->bc_u, 0, 3 * slots * L->real));
   L->bc_bytes = cells.size() * sizeof(uint32_t) + 7 * slots * L->real;
   L->device_bytes += L->bc_bytes;
-  OLB_CUDA(cudaMemcpy(L->bc_cells, cells.data(), cells.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  if (!cells.empty())
+    OLB_CUDA(cudaMemcpy(L->bc_cells, cells.data(), cells.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
   return upload_boundary_values(L);
 }
 
@@ -537,10 +620,11 @@ olb_b200_status boundary_noise(olb_b200_lattice* L)
 template <class R>
 void attach_boundary(const olb_b200_lattice* L, int k, const olb_b200_dyn_params& in, DynDevice<R>& d)
 {
-  if (!is_interpolated(in.kind)) return;
+  if (!has_values(in.kind)) return;
   const auto& b = L->bc_box[size_t(k)];
   d.bc_dir = in.direction;
   d.bc_orient = in.orientation;
+  for (int e = 0; e < 3; ++e) d.nrm[e] = in.normal[e];
   for (int e = 0; e < 6; ++e) d.box[e] = b.box[e];
   d.bc_values = L->bc_values ? static_cast<const R*>(L->bc_values) + 4 * b.slot0 : nullptr;
   d.bc_u = L->bc_u ? static_cast<R*>(L->bc_u) + 3 * b.slot0 : nullptr;
@@ -671,17 +755,35 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
   int bulk = -1, first_bc = -1;
   for (int k = 0; k < n_entries; ++k) {
     const int kind = table[k].kind;
-    if (kind < OLB_B200_DYN_NONE || kind > OLB_B200_DYN_INTERPOLATED_PRESSURE)
+    if (kind < OLB_B200_DYN_NONE || kind > OLB_B200_DYN_VELOCITY_CORNER)
       return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d has unknown kind %d", k, kind);
-    if (is_interpolated(kind)) {
+    if (table[k].reserved != 0)
+      return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d: reserved field must be 0", k);
+    if (has_values(kind)) {
       const int m = table[k].mixin;
       if (m != OLB_B200_DYN_BGK && m != OLB_B200_DYN_TRT && m != OLB_B200_DYN_SMAGORINSKY)
-        return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: entry %d: interpolated boundaries take a BGK, TRT "
+        return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: entry %d: boundaries take a BGK, TRT "
                     "or Smagorinsky-BGK mixin, got kind %d", k, m);
-      if (table[k].direction < 0 || table[k].direction > 2 ||
-          (table[k].orientation != 1 && table[k].orientation != -1))
+      if (kind == OLB_B200_DYN_LOCAL_VELOCITY && m == OLB_B200_DYN_SMAGORINSKY)
+        return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: entry %d: local velocity boundaries with a "
+                    "Smagorinsky-BGK mixin are not implemented", k);
+      if (is_outer(kind)) {
+        int nonzero = 0;
+        bool valid = true;
+        for (int e = 0; e < 3; ++e) {
+          const int v = table[k].normal[e];
+          valid &= v >= -1 && v <= 1;
+          nonzero += v != 0;
+        }
+        if (!valid || nonzero != (kind == OLB_B200_DYN_VELOCITY_EDGE ? 2 : 3))
+          return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d: normal (%d,%d,%d) is not an %s normal", k,
+                      table[k].normal[0], table[k].normal[1], table[k].normal[2],
+                      kind == OLB_B200_DYN_VELOCITY_EDGE ? "edge" : "corner");
+      } else if (table[k].direction < 0 || table[k].direction > 2 ||
+                 (table[k].orientation != 1 && table[k].orientation != -1)) {
         return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d: normal axis %d / sign %d invalid", k,
                     table[k].direction, table[k].orientation);
+      }
       if (!(table[k].omega > 0.0 && table[k].omega < 2.0))
         return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d omega %g outside (0,2)", k, table[k].omega);
       if (first_bc < 0) {
@@ -707,7 +809,7 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
     if (bulk >= 0 && table[bulk].kind != table[first_bc].mixin)
       return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: the boundary mixin (kind %d) must be the lattice's "
                   "fluid collision (kind %d)", table[first_bc].mixin, table[bulk].kind);
-    if (!ids) return fail(OLB_B200_ERR_ARG, "set_dynamics: interpolated boundaries need per-cell ids");
+    if (!ids) return fail(OLB_B200_ERR_ARG, "set_dynamics: boundary entries need per-cell ids");
   }
   bool uniform = ids == nullptr;
   uint8_t first = 0;
@@ -757,6 +859,7 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
   if (!L->masked) {
     std::memcpy(L->bulk, host.data() + only * esz, esz);
   }
+  compute_bulk_box(L, L->masked ? ids : nullptr, bulk);
   L->n_entries = n_entries;
   // a change of kernel class invalidates an earlier tuning
   if (!L->tuned || was_masked != L->masked) {
@@ -856,8 +959,7 @@ olb_b200_status olb_b200_collide_and_stream(olb_b200_lattice* L, int32_t steps, 
     L->flight_pos = (L->flight_pos + 1) % L->flight.size();
   }
   if (!stats) return OLB_B200_OK;
-  const dim3 grid = step_grid(L->g, L->block_z, L->block_y, cells_per_thread(L));
-  const size_t count = size_t(grid.x) * grid.y * grid.z;
+  const size_t count = step_blocks(L) + boundary_blocks(L);
   reduce_partials_kernel<<<1, 1024, 0, L->stream>>>(L->partials, count, L->stat_dev);
   OLB_CUDA(cudaGetLastError());
   OLB_CUDA(cudaMemcpyAsync(L->stat_host, L->stat_dev, sizeof(StatPartial), cudaMemcpyDeviceToHost, L->stream));

@@ -38,9 +38,10 @@ class Dynamics:
     force: tuple = (0.0, 0.0, 0.0)
     wall_u: tuple = (0.0, 0.0, 0.0)
     wall_rho: float = 1.0
-    mixin: int = 0          # interpolated boundaries: the mixin's collision kind
-    direction: int = 0      # interpolated boundaries: outward normal axis
-    orientation: int = 0    # interpolated boundaries: outward normal sign
+    mixin: int = 0          # boundaries: the mixin's collision kind
+    direction: int = 0      # flat boundaries: outward normal axis
+    orientation: int = 0    # flat boundaries: outward normal sign
+    normal: tuple = (0, 0, 0)  # edges and corners: the discrete normal
 
     def params(self, omega_default: float | None = None) -> _abi.DynParams:
         p = _abi.DynParams()
@@ -48,6 +49,8 @@ class Dynamics:
         p.mixin = int(self.mixin)
         p.direction = int(self.direction)
         p.orientation = int(self.orientation)
+        for e in range(3):
+            p.normal[e] = int(self.normal[e])
         omega = self.omega if self.omega is not None else omega_default
         p.omega = float(omega) if omega is not None else 1.0
         p.magic = float(self.magic)
@@ -104,6 +107,28 @@ def InterpolatedPressureBoundary(mixin: Dynamics, direction: int, orientation: i
     src/boundary/interpolatedPressure3D.h:47-90)."""
     return Dynamics(_abi.DYN_INTERPOLATED_PRESSURE, omega=mixin.omega, magic=mixin.magic,
                     smagorinsky=mixin.smagorinsky, mixin=mixin.kind, direction=direction, orientation=orientation)
+
+
+def LocalVelocityBoundary(mixin: Dynamics, direction: int, orientation: int) -> Dynamics:
+    """boundary::LocalVelocity on a flat face (src/boundary/localVelocity3D.h:47-80):
+    CombinedRLBdynamics of the mixin with regularised velocity-boundary momenta."""
+    return Dynamics(_abi.DYN_LOCAL_VELOCITY, omega=mixin.omega, magic=mixin.magic,
+                    smagorinsky=mixin.smagorinsky, mixin=mixin.kind, direction=direction,
+                    orientation=orientation)
+
+
+def VelocityEdgeBoundary(mixin: Dynamics, normal) -> Dynamics:
+    """External edge of a local or interpolated velocity boundary: the mixin with
+    FixedVelocityBoundaryTuple momenta plus OuterVelocityEdgeProcessor3D."""
+    return Dynamics(_abi.DYN_VELOCITY_EDGE, omega=mixin.omega, magic=mixin.magic,
+                    smagorinsky=mixin.smagorinsky, mixin=mixin.kind, normal=tuple(int(v) for v in normal))
+
+
+def VelocityCornerBoundary(mixin: Dynamics, normal) -> Dynamics:
+    """External corner of a local or interpolated velocity boundary: the mixin with
+    FixedVelocityBoundaryTuple momenta plus OuterVelocityCornerProcessor3D."""
+    return Dynamics(_abi.DYN_VELOCITY_CORNER, omega=mixin.omega, magic=mixin.magic,
+                    smagorinsky=mixin.smagorinsky, mixin=mixin.kind, normal=tuple(int(v) for v in normal))
 
 
 FLUID_KINDS = {_abi.DYN_BGK, _abi.DYN_TRT, _abi.DYN_SMAGORINSKY, _abi.DYN_FORCED_BGK, _abi.DYN_FORCED_TRT}

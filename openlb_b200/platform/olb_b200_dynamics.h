@@ -145,6 +145,201 @@ struct Describe<T,DESCRIPTOR,BounceBackVelocity<T,DESCRIPTOR>> {
   }
 };
 
+// --- boundaries (src/boundary/) ----------------------------------------------
+
+/// The mixin collision of a boundary dynamics MIX::exchange_momenta<...>
+template <typename COLLISION>
+struct MixinKind {
+  static constexpr int kind = -1;
+};
+
+template <>
+struct MixinKind<collision::BGK> {
+  static constexpr int kind = OLB_B200_DYN_BGK;
+};
+
+template <>
+struct MixinKind<collision::TRT> {
+  static constexpr int kind = OLB_B200_DYN_TRT;
+};
+
+template <>
+struct MixinKind<collision::SmagorinskyEffectiveOmega<collision::BGK>> {
+  static constexpr int kind = OLB_B200_DYN_SMAGORINSKY;
+};
+
+/// Operator-wide parameters of a boundary's mixin collision, read from the
+/// parameters of the boundary dynamics (which are the mixin's)
+template <typename PARAMETERS_LIST, typename PARAMETERS>
+void mixinParameters(PARAMETERS& parameters, olb_b200_dyn_params& p)
+{
+  p.omega = parameter<descriptors::OMEGA>(parameters);
+  if constexpr (PARAMETERS_LIST::template contains<collision::TRT::MAGIC>()) {
+    p.magic = parameter<collision::TRT::MAGIC>(parameters);
+  }
+  if constexpr (PARAMETERS_LIST::template contains<collision::LES::SMAGORINSKY>()) {
+    p.smagorinsky = parameter<collision::LES::SMAGORINSKY>(parameters);
+  }
+}
+
+/// VELOCITY of FixedVelocityMomentumGeneric (what Cell::defineU sets on
+/// velocity boundary cells, momenta/elements.h:528-560)
+template <typename BLOCK>
+void fixedVelocity(BLOCK& block, CellID iCell, double (&v)[4])
+{
+  const auto u = cellField<momenta::FixedVelocityMomentumGeneric::VELOCITY>(block, iCell, 0.0);
+  v[0] = 1.0;
+  v[1] = u[0];
+  v[2] = u[1];
+  v[3] = u[2];
+}
+
+/// boundary::LocalVelocity on a flat face (src/boundary/localVelocity3D.h:47-80):
+/// CombinedRLBdynamics<MIX, RegularizedVelocityBoundaryTuple<d,o>>
+template <typename T, typename DESCRIPTOR, typename MIX, int d, int o>
+struct Describe<T,DESCRIPTOR,CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::RegularizedVelocityBoundaryTuple<d,o>>> {
+  using DYN = CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::RegularizedVelocityBoundaryTuple<d,o>>;
+  static constexpr int kind = Describe<T,DESCRIPTOR,MIX>::kind >= 0 ? OLB_B200_DYN_LOCAL_VELOCITY : -1;
+  static constexpr bool perCell = false;
+  template <typename PARAMETERS>
+  static void shared(PARAMETERS& parameters, olb_b200_dyn_params& p)
+  {
+    mixinParameters<typename DYN::parameters>(parameters, p);
+    p.mixin = Describe<T,DESCRIPTOR,MIX>::kind;
+    p.direction = d;
+    p.orientation = o;
+  }
+  template <typename BLOCK>
+  static void cell(BLOCK&, CellID, olb_b200_dyn_params&) { }
+};
+
+template <typename T, typename DESCRIPTOR, typename MIX, int d, int o>
+struct BoundaryValues<T,DESCRIPTOR,CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::RegularizedVelocityBoundaryTuple<d,o>>> {
+  static constexpr bool valued = true;
+  template <typename BLOCK>
+  static void get(BLOCK& block, CellID iCell, double (&v)[4])
+  {
+    fixedVelocity(block, iCell, v);
+  }
+};
+
+/// Interpolated velocity on a flat face (src/boundary/interpolatedVelocity3D.h:47-50):
+/// MIX::exchange_momenta<BasicDirichletVelocityBoundaryTuple<d,o>>
+template <typename T, typename DESCRIPTOR, typename EQ, typename COLL, typename COMB, int d, int o>
+struct Describe<T,DESCRIPTOR,dynamics::Tuple<T,DESCRIPTOR,momenta::BasicDirichletVelocityBoundaryTuple<d,o>,EQ,COLL,COMB>> {
+  using DYN = dynamics::Tuple<T,DESCRIPTOR,momenta::BasicDirichletVelocityBoundaryTuple<d,o>,EQ,COLL,COMB>;
+  static constexpr int kind = MixinKind<COLL>::kind >= 0 ? OLB_B200_DYN_INTERPOLATED_VELOCITY : -1;
+  static constexpr bool perCell = false;
+  template <typename PARAMETERS>
+  static void shared(PARAMETERS& parameters, olb_b200_dyn_params& p)
+  {
+    mixinParameters<typename DYN::parameters>(parameters, p);
+    p.mixin = MixinKind<COLL>::kind;
+    p.direction = d;
+    p.orientation = o;
+  }
+  template <typename BLOCK>
+  static void cell(BLOCK&, CellID, olb_b200_dyn_params&) { }
+};
+
+template <typename T, typename DESCRIPTOR, typename EQ, typename COLL, typename COMB, int d, int o>
+struct BoundaryValues<T,DESCRIPTOR,dynamics::Tuple<T,DESCRIPTOR,momenta::BasicDirichletVelocityBoundaryTuple<d,o>,EQ,COLL,COMB>> {
+  static constexpr bool valued = true;
+  template <typename BLOCK>
+  static void get(BLOCK& block, CellID iCell, double (&v)[4])
+  {
+    fixedVelocity(block, iCell, v);
+  }
+};
+
+/// Interpolated pressure on a flat face (src/boundary/interpolatedPressure3D.h:47-90):
+/// MIX::exchange_momenta<BasicDirichletPressureBoundaryTuple<d,o>>
+template <typename T, typename DESCRIPTOR, typename EQ, typename COLL, typename COMB, int d, int o>
+struct Describe<T,DESCRIPTOR,dynamics::Tuple<T,DESCRIPTOR,momenta::BasicDirichletPressureBoundaryTuple<d,o>,EQ,COLL,COMB>> {
+  using DYN = dynamics::Tuple<T,DESCRIPTOR,momenta::BasicDirichletPressureBoundaryTuple<d,o>,EQ,COLL,COMB>;
+  static constexpr int kind = MixinKind<COLL>::kind >= 0 ? OLB_B200_DYN_INTERPOLATED_PRESSURE : -1;
+  static constexpr bool perCell = false;
+  template <typename PARAMETERS>
+  static void shared(PARAMETERS& parameters, olb_b200_dyn_params& p)
+  {
+    mixinParameters<typename DYN::parameters>(parameters, p);
+    p.mixin = MixinKind<COLL>::kind;
+    p.direction = d;
+    p.orientation = o;
+  }
+  template <typename BLOCK>
+  static void cell(BLOCK&, CellID, olb_b200_dyn_params&) { }
+};
+
+template <typename T, typename DESCRIPTOR, typename EQ, typename COLL, typename COMB, int d, int o>
+struct BoundaryValues<T,DESCRIPTOR,dynamics::Tuple<T,DESCRIPTOR,momenta::BasicDirichletPressureBoundaryTuple<d,o>,EQ,COLL,COMB>> {
+  static constexpr bool valued = true;
+  template <typename BLOCK>
+  static void get(BLOCK& block, CellID iCell, double (&v)[4])
+  {
+    // FixedDensity RHO and the tangential velocity of FixedPressureMomentum<d,o>
+    v[0] = cellField<momenta::FixedDensity::RHO>(block, iCell, 1.0)[0];
+    const auto u = cellField<typename momenta::FixedPressureMomentum<d,o>::VELOCITY>(block, iCell, 0.0);
+    v[1] = u[0];
+    v[2] = u[1];
+    v[3] = u[2];
+  }
+};
+
+/// External edges and corners of velocity boundaries (local and
+/// interpolated): MIX::exchange_momenta<FixedVelocityBoundaryTuple>; which of
+/// the two, and the normal, come from the cell's outer post-processor
+template <typename T, typename DESCRIPTOR, typename EQ, typename COLL, typename COMB>
+struct Describe<T,DESCRIPTOR,dynamics::Tuple<T,DESCRIPTOR,momenta::FixedVelocityBoundaryTuple,EQ,COLL,COMB>> {
+  using DYN = dynamics::Tuple<T,DESCRIPTOR,momenta::FixedVelocityBoundaryTuple,EQ,COLL,COMB>;
+  static constexpr int kind = MixinKind<COLL>::kind >= 0 ? kOuterPlaceholder : -1;
+  static constexpr bool perCell = true;
+  template <typename PARAMETERS>
+  static void shared(PARAMETERS& parameters, olb_b200_dyn_params& p)
+  {
+    mixinParameters<typename DYN::parameters>(parameters, p);
+    p.mixin = MixinKind<COLL>::kind;
+  }
+  template <typename BLOCK>
+  static void cell(BLOCK&, CellID, olb_b200_dyn_params&) { }
+};
+
+template <typename T, typename DESCRIPTOR, typename EQ, typename COLL, typename COMB>
+struct BoundaryValues<T,DESCRIPTOR,dynamics::Tuple<T,DESCRIPTOR,momenta::FixedVelocityBoundaryTuple,EQ,COLL,COMB>> {
+  static constexpr bool valued = true;
+  template <typename BLOCK>
+  static void get(BLOCK& block, CellID iCell, double (&v)[4])
+  {
+    fixedVelocity(block, iCell, v);
+  }
+};
+
+/// The boundaries' post-processors, performed by the device step
+template <typename T, typename DESCRIPTOR, int d, int o>
+struct RunsInDeviceStep<PlaneFdBoundaryProcessor3D<T,DESCRIPTOR,d,o>> : std::true_type { };
+
+template <typename T, typename DESCRIPTOR, int plane, int n1, int n2>
+struct RunsInDeviceStep<OuterVelocityEdgeProcessor3D<T,DESCRIPTOR,plane,n1,n2>> : std::true_type { };
+
+template <typename T, typename DESCRIPTOR, int xN, int yN, int zN>
+struct RunsInDeviceStep<OuterVelocityCornerProcessor3D<T,DESCRIPTOR,xN,yN,zN>> : std::true_type { };
+
+/// OuterVelocityEdgeProcessor3D<plane,normal1,normal2>: normal1 along
+/// (plane+1)%3, normal2 along (plane+2)%3 (src/boundary/setBoundary3D.h:586-627)
+template <typename T, typename DESCRIPTOR, int plane, int n1, int n2>
+struct OuterNormal<OuterVelocityEdgeProcessor3D<T,DESCRIPTOR,plane,n1,n2>> {
+  static constexpr int kind = OLB_B200_DYN_VELOCITY_EDGE;
+  static constexpr int normal[3] = {plane == 0 ? 0 : (plane == 1 ? n2 : n1),
+                                    plane == 1 ? 0 : (plane == 2 ? n2 : n1),
+                                    plane == 2 ? 0 : (plane == 0 ? n2 : n1)};
+};
+
+template <typename T, typename DESCRIPTOR, int xN, int yN, int zN>
+struct OuterNormal<OuterVelocityCornerProcessor3D<T,DESCRIPTOR,xN,yN,zN>> {
+  static constexpr int kind = OLB_B200_DYN_VELOCITY_CORNER;
+  static constexpr int normal[3] = {xN, yN, zN};
+};
+
 }
 
 }

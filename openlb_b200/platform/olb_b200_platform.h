@@ -43,9 +43,11 @@
  *    velocity and density, FORCE).  Dynamics the device does not implement
  *    raise std::runtime_error naming them when the table is built; there is
  *    no CPU fallback.
- *  - Post-processors: the statistics post-processor and the interpolated
- *    boundaries' PlaneFdBoundaryProcessor3D run inside the device step; any
- *    other post-processor raises std::runtime_error at set-up.
+ *  - Post-processors: the statistics post-processor, the interpolated
+ *    boundaries' PlaneFdBoundaryProcessor3D and the outer edge and corner
+ *    processors of velocity boundaries run inside the device step (an edge
+ *    or corner processor also tells the device lattice its cell's normal);
+ *    any other post-processor raises std::runtime_error at set-up.
  *
  * Environment (read when a block's device lattice is created):
  *   OLB_B200_DEVICE   CUDA device ordinal (default 0)
@@ -197,6 +199,19 @@ struct Describe {
   static void cell(BLOCK&, CellID, olb_b200_dyn_params&) { }
 };
 
+/// RHO and VELOCITY of a boundary cell (specialised for the boundary
+/// dynamics in olb_b200_dynamics.h); valued == false for all others
+template <typename T, typename DESCRIPTOR, typename DYNAMICS>
+struct BoundaryValues {
+  static constexpr bool valued = false;
+  template <typename BLOCK>
+  static void get(BLOCK&, CellID, double (&v)[4])
+  {
+    v[0] = 1.0;
+    v[1] = v[2] = v[3] = 0.0;
+  }
+};
+
 /// CSE-optimized dynamics (src/cse/wrapper.h) compute what DYNAMICS computes
 template <typename D>
 struct Unwrap {
@@ -246,7 +261,25 @@ struct DeviceDynamics {
   /// Fills the per-cell values (FORCE, wall VELOCITY / RHO)
   virtual void cell(ConcreteBlockLattice<T,DESCRIPTOR,Platform::GPU_B200>& block, CellID iCell,
                     olb_b200_dyn_params& p) = 0;
+  /// Boundary cells (interpolated, local velocity, edges, corners): RHO and
+  /// VELOCITY of the cell as defineRho / defineU set them
+  virtual bool valued() const = 0;
+  virtual void values(ConcreteBlockLattice<T,DESCRIPTOR,Platform::GPU_B200>& block, CellID iCell,
+                      double (&v)[4]) = 0;
 };
+
+/// Kind of a post-processor that marks an external edge or corner of a
+/// velocity boundary, with its discrete normal (specialised in
+/// olb_b200_dynamics.h for OuterVelocityEdgeProcessor3D / CornerProcessor3D)
+template <typename OPERATOR>
+struct OuterNormal {
+  static constexpr int kind = -1;
+  static constexpr int normal[3] = {0, 0, 0};
+};
+
+/// Table kind placeholder of FixedVelocityBoundaryTuple cells: the cell's
+/// edge or corner post-processor decides which one it is and its normal
+constexpr int kOuterPlaceholder = 1000;
 
 /// Device twin of one GPU_B200 block: owns the olb_b200_lattice
 template <typename T, typename DESCRIPTOR>
@@ -262,6 +295,8 @@ private:
   std::vector<olb_b200_dyn_params> _sharedAtUpload;
   std::uint64_t _epochAtUpload = ~std::uint64_t(0);
   bool _onDevice = false;
+  /// external edge / corner cells announced by their post-processors: kind, normal
+  std::unordered_map<CellID, std::array<int,4>> _outer;
 
   static olb_b200_dyn_params blank()
   {
@@ -318,6 +353,8 @@ private:
   /// Per-cell dynamics ids and the entries they index, from the host's dynamics map
   std::vector<std::uint8_t> _ids;
   std::vector<olb_b200_dyn_params> _table;
+  std::vector<std::int64_t> _valueCells;  // boundary cells with values, logical index
+  std::vector<double> _values;            // 4 per cell: RHO, VELOCITY x, y, z
 
   void buildTable()
   {
@@ -343,6 +380,8 @@ private:
     std::uint8_t lastSharedId = 0;
     bool lastSharedValid = false;
     std::size_t n = 0;
+    _valueCells.clear();
+    _values.clear();
     for (int iX = 0; iX < nx; ++iX) {
       for (int iY = 0; iY < ny; ++iY) {
         for (int iZ = 0; iZ < nz; ++iZ, ++n) {
@@ -361,13 +400,30 @@ private:
                                        + " has no device implementation on this platform");
             }
           }
-          if (!lastOp->perCell() && lastSharedValid) {
+          if (!lastOp->perCell() && !lastOp->valued() && lastSharedValid) {
             ids[n] = lastSharedId;
             continue;
           }
           olb_b200_dyn_params p = shared[lastOp];
           if (lastOp->perCell()) {
             lastOp->cell(*_block, iCell, p);
+          }
+          if (p.kind == kOuterPlaceholder) {
+            auto it = _outer.find(iCell);
+            if (it == _outer.end()) {
+              throw std::runtime_error("GPU_B200: a fixed-velocity boundary cell without an outer edge or corner "
+                                       "post-processor (" + lastOp->name() + ")");
+            }
+            p.kind = it->second[0];
+            for (int iD = 0; iD < 3; ++iD) {
+              p.normal[iD] = it->second[1 + iD];
+            }
+          }
+          if (lastOp->valued()) {
+            double v[4];
+            lastOp->values(*_block, iCell, v);
+            _valueCells.push_back(std::int64_t(n));
+            _values.insert(_values.end(), v, v + 4);
           }
           const std::string key(reinterpret_cast<const char*>(&p), sizeof p);
           auto found = entryOf.find(key);
@@ -398,8 +454,16 @@ private:
 
   void uploadDynamics()
   {
-    check(olb_b200_set_dynamics(_handle, _table.size() == 1 ? nullptr : _ids.data(), _table.data(),
+    bool needIds = _table.size() > 1;
+    for (const auto& e : _table) {
+      needIds |= e.kind >= OLB_B200_DYN_INTERPOLATED_VELOCITY;
+    }
+    check(olb_b200_set_dynamics(_handle, needIds ? _ids.data() : nullptr, _table.data(),
                                 int32_t(_table.size())), "set_dynamics");
+    if (!_valueCells.empty()) {
+      check(olb_b200_set_boundary_values(_handle, _valueCells.data(), std::int64_t(_valueCells.size()),
+                                         _values.data()), "set_boundary_values");
+    }
   }
 
   /// Re-uploads the table when setParameter changed an operator-wide parameter
@@ -498,6 +562,13 @@ public:
   void enroll(DeviceDynamics<T,DESCRIPTOR>* op)
   {
     _operators.push_back(op);
+  }
+
+  /// An external edge or corner cell, announced by its post-processor
+  void setOuter(CellID iCell, int kind, const int (&normal)[3])
+  {
+    _outer[iCell] = {kind, normal[0], normal[1], normal[2]};
+    dynamicsEpoch().fetch_add(1, std::memory_order_relaxed);
   }
 
   void setPeriodic(int axis)
@@ -684,18 +755,39 @@ public:
   {
     describe_t::cell(block, iCell, p);
   }
+  bool valued() const override
+  {
+    return gpu::b200::BoundaryValues<T,DESCRIPTOR,typename gpu::b200::Unwrap<DYNAMICS>::type>::valued;
+  }
+  void values(ConcreteBlockLattice<T,DESCRIPTOR,Platform::GPU_B200>& block, CellID iCell,
+              double (&v)[4]) override
+  {
+    gpu::b200::BoundaryValues<T,DESCRIPTOR,typename gpu::b200::Unwrap<DYNAMICS>::type>::get(block, iCell, v);
+  }
 };
 
 namespace gpu {
 
 namespace b200 {
 
-/// Post-processors the fused device step performs itself
+/// Post-processors the fused device step performs itself (the boundary
+/// post-processors are added in olb_b200_dynamics.h)
 template <typename OPERATOR>
 struct RunsInDeviceStep : std::false_type { };
 
 template <>
 struct RunsInDeviceStep<StatisticsPostProcessor> : std::true_type { };
+
+/// CSE-optimized post-processors (src/cse/wrapper.h) compute what OPERATOR computes
+template <typename OPERATOR>
+struct UnwrapOperator {
+  using type = OPERATOR;
+};
+
+template <typename OPERATOR, typename D>
+struct UnwrapOperator<CSE_O<OPERATOR,D>> {
+  using type = OPERATOR;
+};
 
 }
 
@@ -707,7 +799,11 @@ template <typename T, typename DESCRIPTOR, typename OPERATOR, OperatorScope SCOP
 class ConcreteBlockO<T,DESCRIPTOR,Platform::GPU_B200,OPERATOR,SCOPE> final
   : public BlockO<T,DESCRIPTOR,Platform::GPU_B200> {
 private:
+  using op_t = typename gpu::b200::UnwrapOperator<OPERATOR>::type;
+  using outer_t = gpu::b200::OuterNormal<op_t>;
+
   std::size_t _cells = 0;
+  gpu::b200::DeviceLattice<T,DESCRIPTOR>* _device = nullptr;
 
 public:
   std::type_index id() const override
@@ -715,19 +811,23 @@ public:
     return typeid(OPERATOR);
   }
 
-  void set(CellID, bool state) override
+  void set(CellID iCell, bool state) override
   {
     if (state) {
       ++_cells;
+      if constexpr (outer_t::kind >= 0) {
+        _device->setOuter(iCell, outer_t::kind, outer_t::normal);
+      }
     }
   }
 
-  void setup(ConcreteBlockLattice<T,DESCRIPTOR,Platform::GPU_B200>&) override
+  void setup(ConcreteBlockLattice<T,DESCRIPTOR,Platform::GPU_B200>& block) override
   {
-    if constexpr (!gpu::b200::RunsInDeviceStep<OPERATOR>::value) {
+    if constexpr (!gpu::b200::RunsInDeviceStep<op_t>::value) {
       throw std::runtime_error("GPU_B200: post-processor " + fields::name<OPERATOR>()
                                + " has no device implementation on this platform");
     }
+    _device = &gpu::b200::DeviceLattice<T,DESCRIPTOR>::of(block);
   }
 
   void apply(ConcreteBlockLattice<T,DESCRIPTOR,Platform::GPU_B200>&) override { }

@@ -38,7 +38,16 @@ enum {
   /* flat-face interpolated boundaries: the mixin collision with exchanged
    * momenta, plus PlaneFdBoundaryProcessor3D after every stream */
   ORACLE_INTERP_VELOCITY = 8,      /* boundary::InterpolatedVelocity  boundary/interpolatedVelocity3D.h:44-50,78-81 */
-  ORACLE_INTERP_PRESSURE = 9       /* boundary::InterpolatedPressure  boundary/interpolatedPressure3D.h:47-90 */
+  ORACLE_INTERP_PRESSURE = 9,      /* boundary::InterpolatedPressure  boundary/interpolatedPressure3D.h:47-90 */
+  /* flat-face local velocity boundary: CombinedRLBdynamics<MIXIN,
+   * RegularizedVelocityBoundaryTuple<direction,orientation>>, no post-processor */
+  ORACLE_LOCAL_VELOCITY = 10,      /* boundary::LocalVelocity (Flat)  boundary/localVelocity3D.h:47-80 */
+  /* external edges and corners of velocity boundaries (local and
+   * interpolated): MIXIN::exchange_momenta<FixedVelocityBoundaryTuple> plus
+   * OuterVelocityEdgeProcessor3D (priority 0) / OuterVelocityCornerProcessor3D
+   * (priority 1) after every stream; normal[] is the discrete normal */
+  ORACLE_VELOCITY_EDGE = 11,       /* boundary/localVelocity3D.h:90-93,113-114; interpolatedVelocity3D.h:62-63,85-87 */
+  ORACLE_VELOCITY_CORNER = 12      /* boundary/localVelocity3D.h:82-85,111-112; interpolatedVelocity3D.h:54-55,81-83 */
 };
 
 typedef struct {
@@ -50,8 +59,10 @@ typedef struct {
   double force[3];     /* FORCE field value (Guo forcing) */
   double wall_u[3];    /* VELOCITY field of moving-wall bounce-back */
   double wall_rho;     /* FixedDensity RHO field (1 after initialize) */
-  int32_t direction;   /* interpolated boundaries: axis of the outward normal */
-  int32_t orientation; /* interpolated boundaries: its sign, -1 or +1 */
+  int32_t direction;   /* flat boundaries: axis of the outward normal */
+  int32_t orientation; /* flat boundaries: its sign, -1 or +1 */
+  int32_t normal[3];   /* edges and corners: the discrete normal (components -1, 0, +1) */
+  int32_t reserved;
 } oracle_dyn;
 
 typedef struct {
@@ -83,8 +94,9 @@ int oracle_step_f64(const oracle_lattice* lat, double* pops, int steps, double g
                     oracle_stats* stats);
 
 /* The PostStream post-processors alone (PlaneFdBoundaryProcessor3D on every
- * interpolated cell), as BlockLattice::initialize() runs them once on the
- * initial state (core/blockLattice.hh:56-67) before the first collision. */
+ * interpolated cell, then the outer edge and corner processors), as
+ * BlockLattice::initialize() runs them once on the initial state
+ * (core/blockLattice.hh:56-67) before the first collision. */
 int oracle_post_process_f32(const oracle_lattice* lat, float* pops);
 int oracle_post_process_f64(const oracle_lattice* lat, double* pops);
 

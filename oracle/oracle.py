@@ -25,14 +25,17 @@ LIB_PATH = HERE / "_build" / "libolb_oracle.so"
 REF_DIR = HERE / "_ref"
 
 (NONE, BGK, TRT, SMAGORINSKY, BOUNCE_BACK, BOUNCE_BACK_VELOCITY, FORCED_BGK, FORCED_TRT,
- INTERP_VELOCITY, INTERP_PRESSURE) = range(10)
+ INTERP_VELOCITY, INTERP_PRESSURE, LOCAL_VELOCITY, VELOCITY_EDGE, VELOCITY_CORNER) = range(13)
 KIND_NAMES = {
     NONE: "none", BGK: "bgk", TRT: "trt", SMAGORINSKY: "smagorinsky",
     BOUNCE_BACK: "bounce_back", BOUNCE_BACK_VELOCITY: "bounce_back_velocity",
     FORCED_BGK: "forced_bgk", FORCED_TRT: "forced_trt",
     INTERP_VELOCITY: "interpolated_velocity", INTERP_PRESSURE: "interpolated_pressure",
+    LOCAL_VELOCITY: "local_velocity",
 }
 INTERPOLATED = (INTERP_VELOCITY, INTERP_PRESSURE)
+# cells whose boundary values (RHO, VELOCITY) come from bc_values
+VALUED = (INTERP_VELOCITY, INTERP_PRESSURE, LOCAL_VELOCITY, VELOCITY_EDGE, VELOCITY_CORNER)
 
 
 class _Dyn(ctypes.Structure):
@@ -42,6 +45,7 @@ class _Dyn(ctypes.Structure):
         ("smagorinsky", ctypes.c_double), ("force", ctypes.c_double * 3),
         ("wall_u", ctypes.c_double * 3), ("wall_rho", ctypes.c_double),
         ("direction", ctypes.c_int32), ("orientation", ctypes.c_int32),
+        ("normal", ctypes.c_int32 * 3), ("reserved", ctypes.c_int32),
     ]
 
 
@@ -69,9 +73,12 @@ class Dynamics:
     force: tuple = (0.0, 0.0, 0.0)
     wall_u: tuple = (0.0, 0.0, 0.0)
     wall_rho: float = 1.0
-    mixin: int = BGK          # interpolated boundaries: collision of the mixin dynamics
-    direction: int = 0        # interpolated boundaries: outward normal axis
-    orientation: int = -1     # interpolated boundaries: outward normal sign
+    mixin: int = BGK          # boundaries: collision of the mixin dynamics
+    direction: int = 0        # flat boundaries: outward normal axis
+    orientation: int = -1     # flat boundaries: outward normal sign
+    normal: tuple = (0, 0, 0)  # edges and corners: the discrete normal
+    boundary: int = LOCAL_VELOCITY  # edges and corners: the setter they come from
+                                    # (LOCAL_VELOCITY or INTERP_VELOCITY)
 
 
 @dataclass
@@ -120,6 +127,8 @@ def _lattice(case: Case, keep: list):
         table[k].mixin = d.mixin
         table[k].direction = d.direction
         table[k].orientation = d.orientation
+        for e in range(3):
+            table[k].normal[e] = int(d.normal[e])
     lat = _Lattice()
     lat.q = case.q
     lat.nx, lat.ny, lat.nz = case.size
@@ -252,11 +261,13 @@ def write_case(dirpath: Path, case: Case, steps: int, init: np.ndarray | None = 
     lines = [f"size {case.size[0]} {case.size[1]} {case.size[2]}",
              "periodic {} {} {}".format(*[int(bool(p)) for p in case.periodic])]
     omegas = {d.omega for d in case.table
-              if d.kind in (BGK, TRT, SMAGORINSKY, FORCED_BGK, FORCED_TRT) + INTERPOLATED}
+              if d.kind in (BGK, TRT, SMAGORINSKY, FORCED_BGK, FORCED_TRT) + VALUED}
     if len(omegas) > 1:
         raise ValueError("the reference driver takes one lattice-wide OMEGA")
     for k, d in enumerate(case.table):
-        lines.append(f"dyn {k + 1} {KIND_NAMES[d.kind]}")
+        # edge and corner entries are cells of their boundary setter's material
+        name = KIND_NAMES[d.boundary] if d.kind in (VELOCITY_EDGE, VELOCITY_CORNER) else KIND_NAMES[d.kind]
+        lines.append(f"dyn {k + 1} {name}")
         if d.kind == BOUNCE_BACK_VELOCITY:
             lines.append("velocity {} {!r} {!r} {!r}".format(k + 1, *d.wall_u))
         if d.kind in (FORCED_BGK, FORCED_TRT):
@@ -267,10 +278,10 @@ def write_case(dirpath: Path, case: Case, steps: int, init: np.ndarray | None = 
     lines.append(f"omega {ref.omega!r}")
     lines.append(f"magic {ref.magic!r}")
     lines.append(f"smagorinsky {ref.smagorinsky!r}")
-    mixins = {d.mixin for d in case.table if d.kind in INTERPOLATED}
+    mixins = {d.mixin for d in case.table if d.kind in VALUED}
     if mixins:
         if len(mixins) > 1:
-            raise ValueError("the reference driver takes one mixin dynamics for all interpolated boundaries")
+            raise ValueError("the reference driver takes one mixin dynamics for all boundaries")
         lines.append(f"bcmixin {KIND_NAMES[mixins.pop()]}")
         vals = case.bc_values if case.bc_values is not None else np.concatenate(
             [np.ones(case.n), np.zeros(3 * case.n)])

@@ -32,8 +32,10 @@
  *                   `normals 2` stops after writing it)
  *
  * Interpolated boundaries (`dyn <m> interpolated_velocity|interpolated_pressure`)
- * are set like the examples do, boundary::set<InterpolatedVelocity<T,D,MIXIN>>
- * (boundary/setBoundary.h:150-157, boundary/interpolatedVelocity3D.h:36-98),
+ * and local velocity boundaries (`dyn <m> local_velocity`) are set like the
+ * examples do, boundary::set<InterpolatedVelocity<T,D,MIXIN>> or
+ * boundary::set<LocalVelocity<T,D,MIXIN>> (boundary/setBoundary.h:150-157,
+ * boundary/interpolatedVelocity3D.h:36-98, boundary/localVelocity3D.h:36-120),
  * with the fluid material 1 and the outside material 0; MIXIN is the bulk
  * dynamics named by `bcmixin`.  Their boundary values go through Cell::defineRho
  * and Cell::defineU (core/cell.h:194-198).
@@ -154,9 +156,11 @@ void define(SuperLattice<T,DESCRIPTOR>& lattice, SuperGeometry<T,3>& geometry, i
   lattice.template defineDynamics<DYN>(geometry, m);
 }
 
+// boundary conditions set with boundary::set<...> (per-cell discrete normals,
+// per-cell boundary values through defineRho / defineU)
 bool is_interpolated(const std::string& kind)
 {
-  return kind == "interpolated_velocity" || kind == "interpolated_pressure";
+  return kind == "interpolated_velocity" || kind == "interpolated_pressure" || kind == "local_velocity";
 }
 
 template <typename MIXIN>
@@ -165,6 +169,8 @@ void set_interpolated(SuperLattice<T,DESCRIPTOR>& lattice, SuperGeometry<T,3>& g
 {
   if (kind == "interpolated_velocity") {
     boundary::set<boundary::InterpolatedVelocity<T,DESCRIPTOR,MIXIN>>(lattice, geometry, m);
+  } else if (kind == "local_velocity") {
+    boundary::set<boundary::LocalVelocity<T,DESCRIPTOR,MIXIN>>(lattice, geometry, m);
   } else {
     boundary::set<boundary::InterpolatedPressure<T,DESCRIPTOR,MIXIN>>(lattice, geometry, m);
   }

@@ -130,24 +130,123 @@ def interpolated_channel_case(q, size, mixin=O.BGK, omega=1.6, smagorinsky=0.1, 
                   bc_values=vals.reshape(4, -1))
 
 
+# DiscreteNormalType (src/geometry/discreteNormals.h:33-39)
+FLAT, EXTERNAL_CORNER, INTERNAL_CORNER, EXTERNAL_EDGE, INTERNAL_EDGE = range(5)
+
+
+def boundary_table(materials, normals, setters, bulk, mixin=O.BGK, velocity=None):
+    """Dynamics ids and table of a lattice whose boundary materials are set
+    with boundary::set<...> (src/boundary/setBoundary.h:79-157), from the
+    discrete normals OpenLB itself computed (oracle.reference_normals):
+    one entry per (material, normal type, normal).
+
+    materials: int[nx,ny,nz], 1 = fluid; setters: {material: O.LOCAL_VELOCITY
+    | O.INTERP_VELOCITY | O.INTERP_PRESSURE | O.BOUNCE_BACK}; bulk: kwargs of
+    the fluid entry; velocity: {material: (ux, uy, uz)} boundary velocity.
+    Returns (dyn_id, table, bc_values)."""
+    m = np.asarray(materials).reshape(-1)
+    n = m.size
+    table = [O.Dynamics(mixin, **bulk)]
+    key_to_id = {}
+    ids = np.zeros(n, np.uint8)
+    vals = np.zeros((4, n))
+    vals[0] = 1.0
+    for cell in range(n):
+        mat = int(m[cell])
+        if mat == 1:
+            continue
+        setter = setters[mat]
+        if setter == O.BOUNCE_BACK:
+            key = (mat, "bb")
+            entry = lambda: O.Dynamics(O.BOUNCE_BACK)  # noqa: E731
+        else:
+            typ = int(normals[0, cell])
+            nrm = tuple(int(v) for v in normals[1:, cell])
+            if nrm == (0, 0, 0):
+                raise ValueError(f"cell {cell} of material {mat} has no discrete normal")
+            if typ == FLAT:
+                axis = [a for a in range(3) if nrm[a] != 0][0]
+                key = (mat, typ, axis, nrm[axis])
+                entry = lambda a=axis, o=nrm[axis]: O.Dynamics(  # noqa: E731
+                    setter, mixin=mixin, direction=a, orientation=o, **bulk)
+            elif typ in (EXTERNAL_EDGE, EXTERNAL_CORNER) and setter in (O.LOCAL_VELOCITY, O.INTERP_VELOCITY):
+                kind = O.VELOCITY_EDGE if typ == EXTERNAL_EDGE else O.VELOCITY_CORNER
+                key = (mat, typ, nrm)
+                entry = lambda k=kind, v=nrm: O.Dynamics(  # noqa: E731
+                    k, mixin=mixin, normal=v, boundary=setter, **bulk)
+            else:
+                raise ValueError(f"cell {cell}: normal type {typ} of setter {setter} not covered")
+            if velocity and mat in velocity:
+                vals[1:, cell] = velocity[mat]
+        if key not in key_to_id:
+            key_to_id[key] = len(table)
+            table.append(entry())
+        ids[cell] = key_to_id[key]
+    if len(table) > 256:
+        raise ValueError("more than 256 entries")
+    return ids, table, vals
+
+
+def local_velocity_cavity_case(q, size, omega=1 / 0.692, lid=(0.1, 0.0, 0.0), mixin=O.BGK):
+    """cavity3dBenchmark's default set-up (examples/laminar/cavity3dBenchmark/
+    cavity3d.cpp:40-59,71-76): the box surface is material 2 (walls, u = 0)
+    except the y = max face, edges and corners included, which is material 3
+    (the lid, u = lid); both set with boundary::set<LocalVelocity<T,D,BGK>>.
+    Flat faces, external edges and external corners as OpenLB classifies them."""
+    nx, ny, nz = size
+    mats = np.full(size, 2, np.int32)
+    mats[1:-1, 1:-1, 1:-1] = 1
+    mats[:, -1, :] = 3
+    normals = O.reference_normals(mats, (0, 0, 0), boundary_materials=(2, 3), q=q)
+    ids, table, vals = boundary_table(mats, normals, {2: O.LOCAL_VELOCITY, 3: O.LOCAL_VELOCITY},
+                                      dict(omega=omega), mixin=mixin, velocity={3: lid})
+    return O.Case(q=q, size=size, periodic=(0, 0, 0), dyn_id=ids, table=table, bc_values=vals)
+
+
+def open_inlet_channel_case(q, size, omega=1.6, u0=0.05, mixin=O.BGK, seed=0):
+    """Channel whose whole x = 0 face, rim included, is an interpolated
+    velocity inlet: its rim cells are external edges and corners of the
+    inlet (OuterVelocityEdge/CornerProcessor3D).  Bounce-back walls on the y
+    and z faces, an interpolated pressure outlet on the x = nx-1 face interior.
+    Inlet velocity u0 along x with seeded 2 % fluctuations."""
+    nx, ny, nz = size
+    mats = np.full(size, 1, np.int32)
+    mats[:, 0, :] = mats[:, -1, :] = 2
+    mats[:, :, 0] = mats[:, :, -1] = 2
+    mats[0, :, :] = 3
+    mats[-1, 1:-1, 1:-1] = 4
+    normals = O.reference_normals(mats, (0, 0, 0), boundary_materials=(3, 4), q=q)
+    rng = np.random.default_rng(seed)
+    r = 2 * rng.random((3, ny, nz)) - 1
+    ids, table, vals = boundary_table(mats, normals, {2: O.BOUNCE_BACK, 3: O.INTERP_VELOCITY,
+                                                      4: O.INTERP_PRESSURE},
+                                      dict(omega=omega), mixin=mixin)
+    v = vals.reshape((4,) + tuple(size))
+    v[1, 0] = u0 * (1 + 0.02 * r[0])
+    v[2, 0] = u0 * 0.02 * r[1]
+    v[3, 0] = u0 * 0.02 * r[2]
+    return O.Case(q=q, size=size, periodic=(0, 0, 0), dyn_id=ids, table=table, bc_values=v.reshape(4, -1))
+
+
 def to_abi_table(case):
     """oracle.Case -> openlb_b200 dynamics table (same entries, same ids)."""
     import openlb_b200 as ob
     table = []
     for d in case.table:
         extra = {}
-        if d.kind in O.INTERPOLATED:
-            extra = dict(mixin=d.mixin, direction=d.direction, orientation=d.orientation)
+        if d.kind in O.VALUED:
+            extra = dict(mixin=d.mixin, direction=d.direction, orientation=d.orientation,
+                         normal=tuple(d.normal))
         table.append(ob.Dynamics(kind=d.kind, omega=d.omega, magic=d.magic, smagorinsky=d.smagorinsky,
                                  force=tuple(d.force), wall_u=tuple(d.wall_u), wall_rho=d.wall_rho, **extra))
     return table
 
 
 def boundary_cells_and_values(case):
-    """(cells, values[k, 4]) of the interpolated boundary cells of a case, for
-    Lattice.set_boundary_values."""
+    """(cells, values[k, 4]) of the boundary cells that carry values (RHO,
+    VELOCITY) of a case, for Lattice.set_boundary_values."""
     kinds = np.array([d.kind for d in case.table])
-    cells = np.flatnonzero(np.isin(kinds[case.dyn_id], O.INTERPOLATED))
+    cells = np.flatnonzero(np.isin(kinds[case.dyn_id], O.VALUED))
     return cells, case.bc_values[:, cells].T.copy()
 
 

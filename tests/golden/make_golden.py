@@ -79,6 +79,22 @@ def fixture_cases():
         f0 = C.rest_state(q, case.n, dtype)
         name = f"interp_channel_q{q}_{np.dtype(dtype).name}_{O.KIND_NAMES[mixin]}_sisd"
         out.append((name, case, f0, 30, dtype, "sisd", True))
+    # cavity3dBenchmark's default: LocalVelocity walls and lid (flat faces,
+    # external edges and corners, OuterVelocityEdge/CornerProcessor3D)
+    for q, dtype, variants in ((19, np.float32, ("sisd", "nocse")), (19, np.float64, ("sisd",)),
+                               (27, np.float32, ("sisd",)), (27, np.float64, ("sisd",))):
+        case = C.local_velocity_cavity_case(q, (9, 8, 7))
+        f0 = C.rest_state(q, case.n, dtype)
+        for variant in variants:
+            out.append((f"local_cavity_q{q}_{np.dtype(dtype).name}_{variant}", case, f0, 20, dtype, variant, True))
+    # an interpolated velocity inlet over a whole face: its rim is external
+    # edges and corners of the inlet
+    for q, dtype, mixin in ((19, np.float32, O.BGK), (19, np.float64, O.BGK), (27, np.float64, O.TRT)):
+        case = C.open_inlet_channel_case(q, (10, 7, 6), mixin=mixin, seed=q)
+        f0 = C.rest_state(q, case.n, dtype)
+        for variant in (("sisd", "nocse") if (q == 19 and dtype == np.float32) else ("sisd",)):
+            name = f"open_inlet_q{q}_{np.dtype(dtype).name}_{O.KIND_NAMES[mixin]}_{variant}"
+            out.append((name, case, f0, 15, dtype, variant, True))
     return out
 
 
@@ -226,7 +242,7 @@ def main(only: str | None = None):
             "periodic": np.array(case.periodic, np.int32), "steps": np.int32(steps),
             "dyn_id": case.dyn_id if case.dyn_id is not None else np.zeros(case.n, np.uint8),
             "table": np.array([[d.kind, d.omega, d.magic, d.smagorinsky, *d.force, *d.wall_u, d.wall_rho,
-                                d.mixin, d.direction, d.orientation]
+                                d.mixin, d.direction, d.orientation, *d.normal, d.boundary]
                                for d in case.table], np.float64),
             "init": f0, "pops": ref["pops"], "rho": ref["rho"], "u": ref["u"],
         }

@@ -75,7 +75,8 @@ def test_dyn_params_layout_matches_header():
                      header, re.S).group(1)
     names = re.findall(r"^\s*(?:int32_t|double)\s+(\w+)", body, re.M)
     assert ["kind"] + names == [f for f, _ in _abi.DynParams._fields_]
-    assert ctypes.sizeof(_abi.DynParams) == 4 + 4 + 8 * 10 + 4 + 4
+    # kind, mixin, 10 doubles, direction, orientation, normal[3], reserved
+    assert ctypes.sizeof(_abi.DynParams) == 4 + 4 + 8 * 10 + 4 + 4 + 3 * 4 + 4
 
 
 def test_interpolated_entries_from_dynamics():

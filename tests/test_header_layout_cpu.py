@@ -52,7 +52,7 @@ def test_ctypes_mirrors_match_the_header(tmp_path):
 def test_header_compiles_as_cxx17(tmp_path):
     src = tmp_path / "use.cpp"
     src.write_text('#include "olb_b200.h"\n'
-                   "static_assert(sizeof(olb_b200_dyn_params) == 96, \"ABI v2 dynamics entry\");\n"
+                   "static_assert(sizeof(olb_b200_dyn_params) == 112, \"ABI v3 dynamics entry\");\n"
                    "int probe() { olb_b200_desc d{}; d.q = 19; return olb_b200_abi_version() + d.q; }\n")
     subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", f"-I{HEADER.parent}", str(src)],
                    check=True, capture_output=True, text=True)

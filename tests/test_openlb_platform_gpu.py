@@ -1,7 +1,11 @@
 """OpenLB's own example, unmodified, on Platform::GPU_B200.
 
 examples/laminar/cavity3dBenchmark/cavity3d.cpp is compiled from its original
-source by openlb_b200/platform/Makefile twice: against OpenLB patched with the
+source by openlb_b200/platform/Makefile, in both of its set-ups (bb:
+LID_DRIVEN_BOUNCE_BACK, bounce-back walls and a moving-wall lid; local: the
+default, boundary::set<LocalVelocity> on walls and lid, whose box edges and
+corners get OpenLB's outer edge and corner post-processors), twice each:
+against OpenLB patched with the
 GPU_B200 platform tag (PLATFORMS := CPU_SISD GPU_B200, so the load balancer
 hands every cuboid to the B200 platform and each collideAndStream is one fused
 device step through the C ABI) and as the plain CPU_SISD build.  Both run the
@@ -54,7 +58,7 @@ def _fields(workdir: Path):
     return u.astype(np.float64), p.astype(np.float64)
 
 
-@pytest.mark.parametrize("variant", ["bb"])
+@pytest.mark.parametrize("variant", ["bb", "local"])
 def test_cavity3d_example_on_gpu_b200_matches_cpu_sisd(tmp_path, variant):
     dirs = {k: tmp_path / k for k in ("sisd", "nocse", "b200")}
     for d in dirs.values():
@@ -84,8 +88,9 @@ def test_cavity3d_example_on_gpu_b200_matches_cpu_sisd(tmp_path, variant):
     assert dp <= 2 * dp_own
 
 
-def test_cavity3d_example_reports_device_throughput(tmp_path):
+@pytest.mark.parametrize("variant", ["bb", "local"])
+def test_cavity3d_example_reports_device_throughput(tmp_path, variant):
     """The example's own timer (util::Timer, wall clock) over 200 steps of a
     128^3 cavity: with at most two steps in flight it measures the device."""
-    out = _run("cavity3d_bb_b200", tmp_path, "--size", 128, "--steps", 200, "--no-results")
+    out = _run(f"cavity3d_{variant}_b200", tmp_path, "--size", 128, "--steps", 200, "--no-results")
     assert _mlups(out) > 1000
