@@ -23,6 +23,15 @@ so no L2 flush is needed between steps.
 oracle/_ref, all host threads) on the same workload and metric.
 N > 1 (torchrun): every rank runs an independent replica of the workload
 (weak scaling); value is the total cells*steps over the slowest rank's time.
+
+--workload serve runs the served ensemble instead (the serving layer,
+openlb_b200/serving.py): 2000 lid-driven cavities, sides U{24..96}, Re
+log-uniform in [10, 400], lid speed U[0.05, 0.1], each until its
+velocity-change residual < 1e-7 or 20000 steps, Poisson arrivals, 150 GB
+admission budget.  One JSON line: solves/s and p50/p99 latency of the batched
+server, the same requests through the two plain one-at-a-time loops (one
+collideAndStream per step with statistics, as an OpenLB example drives a
+lattice; and this library's multi-step call per 100 steps) and the ratios.
 """
 from __future__ import annotations
 
@@ -58,6 +67,14 @@ def parse():
     ap.add_argument("--lattice", type=int, default=WORKLOAD["q"], choices=[19, 27])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="step", choices=["step", "serve"],
+                    help="step: the fused step on the 256^3 TGV (default); serve: the served "
+                         "ensemble of cavities against both plain loops")
+    ap.add_argument("--requests", type=int, default=2000, help="serve: number of requests")
+    ap.add_argument("--rate", type=float, default=50.0, help="serve: Poisson arrival rate per s")
+    ap.add_argument("--max-steps", type=int, default=20000, help="serve: step limit per request")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="serve: HBM admission budget")
+    ap.add_argument("--no-plain", action="store_true", help="serve: skip the two plain loops")
     return ap.parse_args()
 
 
@@ -303,10 +320,46 @@ def cpu_threads():
 
 
 # ---------------------------------------------------------------------------
+# the served ensemble (continuous batching) against the plain loops
+
+SERVE = {"name": "serve_cavities", "sides": (24, 96), "re": (10.0, 400.0), "lid": (0.05, 0.1), "tol": 1e-7,
+         "check": 100, "seed": 5}
+
+
+def run_serve(args, world, rank, local):
+    """One JSON line: solves/s and p50/p99 latency of the batched server, the
+    same requests through both plain one-at-a-time loops, and the ratios.
+    Every rank serves its own request stream (replicas); rank 0 reports its
+    own line with the total solves/s of all ranks as value."""
+    from openlb_b200 import serving
+    reqs = serving.make_requests(args.requests, args.rate, SERVE["seed"] + rank, SERVE["sides"], SERVE["re"],
+                                 SERVE["lid"], SERVE["tol"], args.max_steps)
+    b = serving.serve_batched(reqs, int(args.budget_gb * 2 ** 30), 4096, SERVE["check"], device=local)
+    steps = {r.rid: r.steps for r in b["results"]}
+    cell_steps = float(sum(r.cells * steps[r.rid] for r in reqs))
+    out = {"batched": {k: v for k, v in b.items() if k != "results"}}
+    out["batched"]["mlups"] = cell_steps / b["wall_s"] / 1e6
+    if not args.no_plain:
+        for style, key in (("per_step", "plain_per_step"), ("chunked", "plain_chunked")):
+            p = serving.serve_plain(reqs, SERVE["check"], device=local, style=style)
+            out[key] = {k: v for k, v in p.items() if k != "results"}
+            out[key]["mlups"] = cell_steps / p["wall_s"] / 1e6
+            out[f"speedup_vs_{key}"] = b["solves_per_s"] / p["solves_per_s"]
+    total = b["solves_per_s"]
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([total], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t)
+        total = float(t.item())
+    return total, out, cell_steps
+
 
 def main():
     args = parse()
     world, rank, local = dist_init(args)
+    if args.workload == "serve":
+        return main_serve(args, world, rank, local)
     config = {"workload": WORKLOAD["name"] if (args.n, args.lattice, args.storage) == (256, 19, "f32")
               else f"tgv{args.n}_d3q{args.lattice}_bgk_{args.storage}",
               "lattice": f"D3Q{args.lattice}", "cells": args.n ** 3, "size": [args.n] * 3,
@@ -355,6 +408,32 @@ def main():
         else:
             line["cpu_baseline"] = {"value": None, "unavailable": err}
     if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main_serve(args, world, rank, local):
+    config = {"workload": SERVE["name"], "requests": args.requests, "sides": list(SERVE["sides"]),
+              "re_log_uniform": list(SERVE["re"]), "lid": list(SERVE["lid"]), "tol": SERVE["tol"],
+              "max_steps": args.max_steps, "budget_gb": args.budget_gb, "arrivals": f"poisson {args.rate}/s",
+              "seed": SERVE["seed"], "check_interval": SERVE["check"], "lattice": "D3Q19", "collision": "BGK",
+              "storage": "f32", "parallelism": f"replicas{world}" if world > 1 else "single-gpu"}
+    line = {"metric": "solves/s", "unit": "solves/s", "n_gpus": world, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic", "dtype": "f32", "config": config}
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "unavailable": "OpenLB has no serving layer; its "
+                              "one-request-at-a-time loop is the plain_per_step arm of this line"}))
+        return
+    total, out, cell_steps = run_serve(args, world, rank, local)
+    if rank == 0:
+        b = out["batched"]
+        line.update({"value": total, "p50_latency_s": b["p50_latency_s"], "p99_latency_s": b["p99_latency_s"],
+                     "e2e": {"value": total, "unit": "solves/s", "note": "host-driven server, wall clock "
+                             "from the first arrival to the last completion"},
+                     "cell_steps": cell_steps, **out})
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

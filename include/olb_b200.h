@@ -170,6 +170,18 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* lattice, const uint8_t* 
 olb_b200_status olb_b200_set_boundary_values(olb_b200_lattice* lattice, const int64_t* cells, int64_t count,
                                              const double* values);
 
+/* A FORCE value per cell for the Guo-forced dynamics (FORCED_BGK,
+ * FORCED_TRT) in place of their entry's constant force — replaces OpenLB's
+ * per-cell FORCE field (defineField<descriptors::FORCE>, cell.setField;
+ * read by forcing::Guo, src/dynamics/forcing.h:53-69, and by the forced
+ * momenta, src/dynamics/momenta/elements.h:1480-1488).  force holds 3 x cells
+ * values of the ABI element type (double for OLB_B200_STORAGE_F64, float
+ * otherwise), component-major (x of every cell, then y, then z), cells in the
+ * populations' order.  Other dynamics ignore the field.  force == NULL removes
+ * it (the entries' forces apply again).  The step then reads 3 more values per
+ * cell.  Synchronous. */
+olb_b200_status olb_b200_set_force_field(olb_b200_lattice* lattice, const void* force);
+
 /* Per-step fluctuations of the interpolated velocity inlets — what an OpenLB
  * example does by calling defineU with a random field before every step.  No
  * counterpart in the reference's library.  Before step t (t = steps done so

@@ -49,7 +49,7 @@ EXPORTED = [
     "olb_b200_ensemble_remove", "olb_b200_ensemble_run", "olb_b200_ensemble_get_moments",
     "olb_b200_ensemble_info", "olb_b200_ensemble_set_occupancy", "olb_b200_ensemble_bytes_per_instance",
     "olb_b200_set_boundary_values", "olb_b200_initialize", "olb_b200_set_boundary_noise",
-    "olb_b200_set_max_steps_in_flight",
+    "olb_b200_set_max_steps_in_flight", "olb_b200_set_force_field",
 ]
 
 ENSEMBLE_CAVITY, ENSEMBLE_CHANNEL = 1, 2
@@ -160,6 +160,8 @@ def load(variant: str = "fast") -> ctypes.CDLL:
     lib.olb_b200_synchronize.restype = st
     lib.olb_b200_set_max_steps_in_flight.argtypes = [P, ctypes.c_int32]
     lib.olb_b200_set_max_steps_in_flight.restype = st
+    lib.olb_b200_set_force_field.argtypes = [P, ctypes.c_void_p]
+    lib.olb_b200_set_force_field.restype = st
     lib.olb_b200_time_steps.argtypes = [P, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)]
     lib.olb_b200_time_steps.restype = st
     lib.olb_b200_get_stream.argtypes = [P, ctypes.POINTER(P)]

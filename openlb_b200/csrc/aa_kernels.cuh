@@ -39,6 +39,10 @@ struct Geometry {
   // masked lattices: a box [lo, hi) whose cells all use the bulk entry, so the
   // step kernel skips their dynamics id (empty when lo == hi)
   int32_t bulk_lo[3], bulk_hi[3];
+  int32_t bulk_id;  // masked lattices: the table entry of the box cells
+  // FORCE per cell for the Guo-forced dynamics (3 columns of `stride` values
+  // of the compute type, natural cell order), or nullptr: the entries' forces
+  const void* force;
 };
 
 OLB_HD bool in_bulk_box(const Geometry& g, int x, int y, int z)
@@ -209,48 +213,47 @@ constexpr StepVariant kStepVariants[] = {{1, 3}, {1, 4}, {2, 2}, {2, 3}};
 #endif
 constexpr int kNumStepVariants = 4;
 
-template <int Q, class S, class R, int KIND, bool ODD, bool MASKED, bool STATS, int CPT, int MINB>
-__global__ void __launch_bounds__(kStepThreads, MINB)
-aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict__ ids,
-               const DynDevice<R>* __restrict__ table, const DynDevice<R> bulk,
-               StatPartial* __restrict__ partials)
+// running sums of the fused statistics of one thread
+struct StatAcc {
+  double rho = 0., usqr = 0., max = 0.;
+  unsigned long long n = 0, nf = 0;
+  OLB_DEV void add(double r, double u2)
+  {
+    if (isfinite(r) && isfinite(u2)) {
+      rho += r; usqr += u2; max = fmax(max, u2); n += 1;
+    } else {
+      nf += 1;
+    }
+  }
+};
+
+// One tile of the step: the CPT cells (x, y0 + k*dy, z) of this thread.
+// Masked lattices pass each cell's table entry in id[k] (loaded a tile ahead by
+// aa_step_masked_kernel); unmasked lattices use `bulk` for every cell.
+template <int Q, class S, class R, int KIND, bool ODD, bool MASKED, bool STATS, int CPT>
+OLB_DEV void step_tile(S* __restrict__ pops, const Geometry& g, const DynDevice<R>* __restrict__ table,
+                       const DynDevice<R>& bulk, int x, int y0, int z, int dy, const int (&id)[CPT], StatAcc& acc)
 {
   using L = Lattice<Q>;
   using ST = Store<S, R>;
-  const int z = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
-  const int x = blockIdx.z;
-
-  double s_rho = 0., s_usqr = 0., s_max = 0.;
-  unsigned long long s_n = 0, s_nf = 0;
-
+  constexpr bool kForced = KIND == K_FORCED_BGK || KIND == K_FORCED_TRT;
   R f[CPT][Q];
+  R fc[CPT][3];  // the cell's FORCE when the lattice has a force field
   int kind[CPT];
   bool go[CPT];
-  bool inside[CPT];  // masked lattices: in the bulk box, no dynamics id needed
   uint32_t n[CPT];
-  const DynDevice<R>* p[CPT];
 
-  // phase 1: classify the cells and issue all their loads.  Cells of the bulk
-  // box (all cells of an unmasked lattice) need no dynamics id: a warp whose
-  // cells all lie in the box issues its population loads at once, the others
-  // wait for their ids and kinds (full-way bounce-back moves no bytes).
+  // phase 1: classify the cells and issue all their loads (full-way
+  // bounce-back moves no bytes)
   static_for<0, CPT>([&](auto k) {
-    const int y = y0 + k.value * int(blockDim.y);
+    const int y = y0 + k.value * dy;
     go[k] = z < g.nz && y < g.ny;
     kind[k] = KIND;
-    p[k] = nullptr;  // masked lattices: the cell's table entry (box cells use `bulk`)
     n[k] = 0;
-    inside[k] = !MASKED;
     if (go[k]) {
       n[k] = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
       if constexpr (MASKED) {
-        inside[k] = in_bulk_box(g, x, y, z);
-        if (!inside[k]) {
-          const DynDevice<R>* e = table + ids[n[k]];
-          kind[k] = __ldg(&e->kind);
-          p[k] = e;
-        }
+        kind[k] = __ldg(&table[id[k]].kind);
       }
       // full-way bounce-back is a no-op on the AA pattern (see file comment)
       go[k] = kind[k] != K_BOUNCE_BACK;
@@ -266,46 +269,58 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict
           f[k][i] = ST::template load<L, o>(pops + size_t(o) * g.stride + src);
         }
       });
+      if constexpr (kForced) {
+        fc[k][0] = fc[k][1] = fc[k][2] = R(0);
+        if (g.force) {
+          const R* __restrict__ F = static_cast<const R*>(g.force);
+          fc[k][0] = __ldg(F + n[k]);
+          fc[k][1] = __ldg(F + size_t(g.stride) + n[k]);
+          fc[k][2] = __ldg(F + 2 * size_t(g.stride) + n[k]);
+        }
+      }
     }
   });
 
   // phase 2: collide and store
   static_for<0, CPT>([&](auto k) {
     if (!go[k]) return;
-    const int y = y0 + k.value * int(blockDim.y);
+    const int y = y0 + k.value * dy;
     R st_rho = R(0), st_usqr = R(0);
     bool counted = false;
     if (kind[k] == KIND) {
       if constexpr (MASKED) {
-        // the entry's collision constants: the bulk entry's for box cells
+        // the entry's collision constants
+        const DynDevice<R>* e = table + id[k];
         DynDevice<R> q;
-        if (inside[k]) {
-          q.omega = bulk.omega;
-          q.omega_minus = bulk.omega_minus;
-          q.smago_pre = bulk.smago_pre;
-          q.tau_mol = bulk.tau_mol;
-          q.force[0] = bulk.force[0];
-          q.force[1] = bulk.force[1];
-          q.force[2] = bulk.force[2];
-          q.force_relax = bulk.force_relax;
-        } else {
-          const DynDevice<R>* e = p[k];
-          q.omega = __ldg(&e->omega);
-          q.omega_minus = __ldg(&e->omega_minus);
-          q.smago_pre = __ldg(&e->smago_pre);
-          q.tau_mol = __ldg(&e->tau_mol);
-          q.force[0] = __ldg(&e->force[0]);
-          q.force[1] = __ldg(&e->force[1]);
-          q.force[2] = __ldg(&e->force[2]);
-          q.force_relax = __ldg(&e->force_relax);
+        q.omega = __ldg(&e->omega);
+        q.omega_minus = __ldg(&e->omega_minus);
+        q.smago_pre = __ldg(&e->smago_pre);
+        q.tau_mol = __ldg(&e->tau_mol);
+        q.force[0] = __ldg(&e->force[0]);
+        q.force[1] = __ldg(&e->force[1]);
+        q.force[2] = __ldg(&e->force[2]);
+        q.force_relax = __ldg(&e->force_relax);
+        if constexpr (kForced) {
+          if (g.force) {
+            q.force[0] = fc[k][0]; q.force[1] = fc[k][1]; q.force[2] = fc[k][2];
+          }
         }
+        collide_bulk<L, KIND>(f[k], q, st_rho, st_usqr);
+      } else if constexpr (kForced) {
+        DynDevice<R> q;
+        q.omega = bulk.omega;
+        q.omega_minus = bulk.omega_minus;
+        q.force_relax = bulk.force_relax;
+        q.force[0] = g.force ? fc[k][0] : bulk.force[0];
+        q.force[1] = g.force ? fc[k][1] : bulk.force[1];
+        q.force[2] = g.force ? fc[k][2] : bulk.force[2];
         collide_bulk<L, KIND>(f[k], q, st_rho, st_usqr);
       } else {
         collide_bulk<L, KIND>(f[k], bulk, st_rho, st_usqr);
       }
       counted = true;
     } else if (MASKED && kind[k] == K_BOUNCE_BACK_VELOCITY) {
-      const DynDevice<R>* e = p[k];
+      const DynDevice<R>* e = table + id[k];
       revert<L>(f[k]);
       static_for<1, Q>([&](auto i) {
         f[k][i] += __ldg(&e->wall_term[i][0]);
@@ -335,18 +350,102 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict
       }
     });
     if constexpr (STATS) {
-      if (counted) {
-        const double r = double(st_rho), u2 = double(st_usqr);
-        if (isfinite(r) && isfinite(u2)) {
-          s_rho += r; s_usqr += u2; s_max = fmax(s_max, u2); s_n += 1;
-        } else {
-          s_nf += 1;
-        }
-      }
+      if (counted) acc.add(double(st_rho), double(st_usqr));
     }
   });
+}
+
+// Unmasked lattices (every cell uses `bulk`): one tile per block, grid
+// step_grid().
+template <int Q, class S, class R, int KIND, bool ODD, bool STATS, int CPT, int MINB>
+__global__ void __launch_bounds__(kStepThreads, MINB)
+aa_step_kernel(S* __restrict__ pops, const Geometry g, const DynDevice<R> bulk, StatPartial* __restrict__ partials)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
+  const int x = blockIdx.z;
+  const int none[CPT] = {};
+  StatAcc acc;
+  step_tile<Q, S, R, KIND, ODD, false, STATS, CPT>(pops, g, nullptr, bulk, x, y0, z, int(blockDim.y), none, acc);
   if constexpr (STATS) {
-    block_stats(s_rho, s_usqr, s_max, s_n, s_nf, partials);
+    block_stats(acc.rho, acc.usqr, acc.max, acc.n, acc.nf, partials);
+  }
+}
+
+// Tiles of the masked kernels: the blocks of step_grid() in launch order,
+// t = bx + tz * (by + ty * x); origin() gives a thread's first cell in tile t.
+struct TileGrid {
+  uint32_t tz, ty, tiles, rows;
+  OLB_DEV TileGrid(const Geometry& g, int cpt, int nx)
+  {
+    rows = blockDim.y * uint32_t(cpt);
+    tz = (uint32_t(g.nz) + blockDim.x - 1) / blockDim.x;
+    ty = (uint32_t(g.ny) + rows - 1) / rows;
+    tiles = tz * ty * uint32_t(nx);
+  }
+  OLB_DEV void origin(uint32_t t, int& x, int& y0, int& z) const
+  {
+    const uint32_t r = t / tz;
+    const uint32_t xi = r / ty;
+    z = int((t - r * tz) * blockDim.x + threadIdx.x);
+    y0 = int((r - xi * ty) * rows + threadIdx.y);
+    x = int(xi);
+  }
+};
+
+// table entries of a tile's cells: box cells use the bulk entry without a
+// load; cells outside the lattice get -1 (they are skipped)
+template <int CPT>
+OLB_DEV void load_tile_ids(int (&id)[CPT], const Geometry& g, const uint8_t* __restrict__ ids, int x, int y0,
+                           int z, int dy)
+{
+  static_for<0, CPT>([&](auto k) {
+    const int y = y0 + k.value * dy;
+    id[k] = -1;
+    if (z < g.nz && y < g.ny) {
+      id[k] = in_bulk_box(g, x, y, z)
+                ? g.bulk_id
+                : int(ids[(uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z)]);
+    }
+  });
+}
+
+// Masked lattices: a persistent grid of masked_grid() blocks walks the tiles
+// with a stride of gridDim.x.  A cell's dynamics id must be read before its
+// populations can be (bounce-back cells load none), so each block issues the
+// ids of its next tile before the populations of the current one: the id
+// latency overlaps a tile of work instead of preceding every population load.
+template <int Q, class S, class R, int KIND, bool ODD, bool STATS, int CPT, int MINB>
+__global__ void __launch_bounds__(kStepThreads, MINB)
+aa_step_masked_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict__ ids,
+                      const DynDevice<R>* __restrict__ table, const DynDevice<R> bulk,
+                      StatPartial* __restrict__ partials)
+{
+  const TileGrid tg(g, CPT, g.nx);
+  const int dy = int(blockDim.y);
+  StatAcc acc;
+  int next[CPT];
+  uint32_t t = blockIdx.x;
+  if (t < tg.tiles) {
+    int x, y0, z;
+    tg.origin(t, x, y0, z);
+    load_tile_ids(next, g, ids, x, y0, z, dy);
+  }
+  for (; t < tg.tiles; t += gridDim.x) {
+    int cur[CPT];
+    static_for<0, CPT>([&](auto k) { cur[k] = next[k]; });
+    const uint32_t tn = t + gridDim.x;
+    if (tn < tg.tiles) {
+      int xn, yn, zn;
+      tg.origin(tn, xn, yn, zn);
+      load_tile_ids(next, g, ids, xn, yn, zn, dy);
+    }
+    int x, y0, z;
+    tg.origin(t, x, y0, z);
+    step_tile<Q, S, R, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, x, y0, z, dy, cur, acc);
+  }
+  if constexpr (STATS) {
+    block_stats(acc.rho, acc.usqr, acc.max, acc.n, acc.nf, partials);
   }
 }
 
@@ -413,22 +512,40 @@ struct PairNeighbours {
   OLB_DEV uint32_t at() const { return xo[DX + 1] + yo[DY + 1] + zo[DZ + 1]; }
 };
 
-// collision of one cell of a pair by its runtime kind (masked lattices)
+// collision of one cell of a pair by its runtime kind (masked lattices);
+// field: the Guo-forced dynamics take the cell's FORCE from fcell
 template <class L, int KIND, bool MASKED>
 OLB_DEV bool collide_any(float (&f)[L::q], int kind, const DynDevice<float>* e, const DynDevice<float>& bulk,
-                         int x, int y, int z, float& st_rho, float& st_usqr)
+                         const float (&fcell)[3], bool field, float& st_rho, float& st_usqr)
 {
+  constexpr bool kForced = KIND == K_FORCED_BGK || KIND == K_FORCED_TRT;
   if (kind == KIND) {
-    if (MASKED && e) {
+    if ((MASKED && e) || (kForced && field)) {
       DynDevice<float> q;
-      q.omega = __ldg(&e->omega);
-      q.omega_minus = __ldg(&e->omega_minus);
-      q.smago_pre = __ldg(&e->smago_pre);
-      q.tau_mol = __ldg(&e->tau_mol);
-      q.force[0] = __ldg(&e->force[0]);
-      q.force[1] = __ldg(&e->force[1]);
-      q.force[2] = __ldg(&e->force[2]);
-      q.force_relax = __ldg(&e->force_relax);
+      if (MASKED && e) {
+        q.omega = __ldg(&e->omega);
+        q.omega_minus = __ldg(&e->omega_minus);
+        q.smago_pre = __ldg(&e->smago_pre);
+        q.tau_mol = __ldg(&e->tau_mol);
+        q.force[0] = __ldg(&e->force[0]);
+        q.force[1] = __ldg(&e->force[1]);
+        q.force[2] = __ldg(&e->force[2]);
+        q.force_relax = __ldg(&e->force_relax);
+      } else {
+        q.omega = bulk.omega;
+        q.omega_minus = bulk.omega_minus;
+        q.smago_pre = bulk.smago_pre;
+        q.tau_mol = bulk.tau_mol;
+        q.force[0] = bulk.force[0];
+        q.force[1] = bulk.force[1];
+        q.force[2] = bulk.force[2];
+        q.force_relax = bulk.force_relax;
+      }
+      if constexpr (kForced) {
+        if (field) {
+          q.force[0] = fcell[0]; q.force[1] = fcell[1]; q.force[2] = fcell[2];
+        }
+      }
       collide_bulk<L, KIND>(f, q, st_rho, st_usqr);
     } else {
       collide_bulk<L, KIND>(f, bulk, st_rho, st_usqr);
@@ -454,24 +571,20 @@ OLB_DEV bool collide_any(float (&f)[L::q], int kind, const DynDevice<float>* e, 
   return false;  // NoDynamics / bounce-back / boundary cells (collided ahead): no statistic here
 }
 
-template <int Q, class S, int KIND, bool ODD, bool MASKED, bool STATS, int CPT, int MINB>
-__global__ void __launch_bounds__(kStepThreads, MINB)
-aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8_t* __restrict__ ids,
-                      const DynDevice<float>* __restrict__ table, const DynDevice<float> bulk,
-                      StatPartial* __restrict__ partials)
+// One tile of the paired step: the CPT element rows (x', y0 + k*dy, z) of
+// this thread, each the two cells x' and x' + nx/2.  Masked lattices pass the
+// table entries of both cells (loaded a tile ahead); unmasked ones use `bulk`.
+template <int Q, class S, int KIND, bool ODD, bool MASKED, bool STATS, int CPT>
+OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const DynDevice<float>* __restrict__ table,
+                         const DynDevice<float>& bulk, int xp, int y0, int z, int dy, const int (&id_lo)[CPT],
+                         const int (&id_hi)[CPT], StatAcc& acc)
 {
   using L = Lattice<Q>;
   using P = Pair<S>;
   using T = typename P::T;
+  constexpr bool kForced = KIND == K_FORCED_BGK || KIND == K_FORCED_TRT;
   T* __restrict__ pops = reinterpret_cast<T*>(pops_scalar);
   const uint32_t pstride = g.stride >> 1;  // elements per column
-  const int z = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
-  const int xp = blockIdx.z;
-  const uint32_t half_cells = uint32_t(g.nx >> 1) * uint32_t(g.ny) * uint32_t(g.nz);
-
-  double s_rho = 0., s_usqr = 0., s_max = 0.;
-  unsigned long long s_n = 0, s_nf = 0;
 
   // the loaded pairs stay packed (low half = cell x', high half = x' + nx/2):
   // one 32-bit register per population for both cells
@@ -479,25 +592,17 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
   int kind_lo[CPT], kind_hi[CPT];
   bool go[CPT];
   uint32_t e[CPT];
-  const DynDevice<float>* p_lo[CPT];
-  const DynDevice<float>* p_hi[CPT];
 
   static_for<0, CPT>([&](auto k) {
-    const int y = y0 + k.value * int(blockDim.y);
+    const int y = y0 + k.value * dy;
     go[k] = z < g.nz && y < g.ny;
     kind_lo[k] = kind_hi[k] = KIND;
-    p_lo[k] = p_hi[k] = nullptr;  // nullptr: the bulk entry (kernel argument)
     e[k] = 0;
     if (go[k]) {
       e[k] = (uint32_t(xp) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
       if constexpr (MASKED) {
-        // both cells in the bulk box: the bulk entry, no dynamics ids
-        if (!(in_bulk_box(g, xp, y, z) && in_bulk_box(g, xp + (g.nx >> 1), y, z))) {
-          p_lo[k] = table + ids[e[k]];
-          p_hi[k] = table + ids[e[k] + half_cells];
-          kind_lo[k] = __ldg(&p_lo[k]->kind);
-          kind_hi[k] = __ldg(&p_hi[k]->kind);
-        }
+        kind_lo[k] = __ldg(&table[id_lo[k]].kind);
+        kind_hi[k] = __ldg(&table[id_hi[k]].kind);
       }
       // two bounce-back cells: nothing to do (AA no-op)
       go[k] = !(kind_lo[k] == K_BOUNCE_BACK && kind_hi[k] == K_BOUNCE_BACK);
@@ -525,7 +630,7 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
 
   static_for<0, CPT>([&](auto k) {
     if (!go[k]) return;
-    const int y = y0 + k.value * int(blockDim.y);
+    const int y = y0 + k.value * dy;
     // Both cells of the pair are collided in the scaled representation
     // g_i = s_i (f_i - w_i) of the storage, one after the other.  BGK and
     // TRT cells collide on g directly (relax_*_scaled); any other dynamics
@@ -547,18 +652,42 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
       });
       float r = 0.f, u2 = 0.f;
       bool counted = false, done = false;
+      // the cell's FORCE when the lattice has a force field (Guo-forced
+      // dynamics; loaded here, after the populations)
+      float fcell[3] = {0.f, 0.f, 0.f};
+      const bool field = kForced && g.force != nullptr;
+      if constexpr (kForced) {
+        if (field && (!MASKED || kind == KIND)) {
+          const float* __restrict__ F = static_cast<const float*>(g.force);
+          const uint32_t nn = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
+          fcell[0] = __ldg(F + nn);
+          fcell[1] = __ldg(F + size_t(g.stride) + nn);
+          fcell[2] = __ldg(F + 2 * size_t(g.stride) + nn);
+        }
+      }
 #ifndef OLB_B200_EXACT
       if (!MASKED || kind == KIND) {
-        if (MASKED && pe) {
+        if ((MASKED && pe) || field) {
           DynDevice<float> q;
-          q.omega = __ldg(&pe->omega);
-          q.omega_minus = __ldg(&pe->omega_minus);
-          q.smago_pre = __ldg(&pe->smago_pre);
-          q.tau_mol = __ldg(&pe->tau_mol);
-          q.force[0] = __ldg(&pe->force[0]);
-          q.force[1] = __ldg(&pe->force[1]);
-          q.force[2] = __ldg(&pe->force[2]);
-          q.force_relax = __ldg(&pe->force_relax);
+          if (MASKED && pe) {
+            q.omega = __ldg(&pe->omega);
+            q.omega_minus = __ldg(&pe->omega_minus);
+            q.smago_pre = __ldg(&pe->smago_pre);
+            q.tau_mol = __ldg(&pe->tau_mol);
+            q.force[0] = __ldg(&pe->force[0]);
+            q.force[1] = __ldg(&pe->force[1]);
+            q.force[2] = __ldg(&pe->force[2]);
+            q.force_relax = __ldg(&pe->force_relax);
+          } else {
+            q.omega = bulk.omega;
+            q.omega_minus = bulk.omega_minus;
+            q.smago_pre = bulk.smago_pre;
+            q.tau_mol = bulk.tau_mol;
+            q.force_relax = bulk.force_relax;
+          }
+          if (field) {
+            q.force[0] = fcell[0]; q.force[1] = fcell[1]; q.force[2] = fcell[2];
+          }
           collide_scaled<L, KIND>(gout, q, r, u2);
         } else {
           collide_scaled<L, KIND>(gout, bulk, r, u2);
@@ -572,7 +701,7 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
           constexpr float inv = 1.f / storage_scale<L>(i);
           gout[i] *= inv;
         });
-        counted = collide_any<L, KIND, MASKED>(gout, kind, pe, bulk, x, y, z, r, u2);
+        counted = collide_any<L, KIND, MASKED>(gout, kind, pe, bulk, fcell, field, r, u2);
         static_for<0, Q>([&](auto i) {
           constexpr float sc = storage_scale<L>(i);
           gout[i] *= sc;
@@ -592,15 +721,12 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
         }
       });
       if constexpr (STATS) {
-        if (counted) {
-          const double rr = r, uu = u2;
-          if (isfinite(rr) && isfinite(uu)) { s_rho += rr; s_usqr += uu; s_max = fmax(s_max, uu); s_n += 1; }
-          else { s_nf += 1; }
-        }
+        if (counted) acc.add(double(r), double(u2));
       }
     };
-    cell(std::integral_constant<bool, false>{}, kind_lo[k], p_lo[k]);
-    cell(std::integral_constant<bool, true>{}, kind_hi[k], p_hi[k]);
+    // the table entries (nullptr: the bulk entry, the kernel argument)
+    cell(std::integral_constant<bool, false>{}, kind_lo[k], MASKED ? table + id_lo[k] : nullptr);
+    cell(std::integral_constant<bool, true>{}, kind_hi[k], MASKED ? table + id_hi[k] : nullptr);
     // recomputed after the collision rather than kept live through it
     PairNeighbours nb(g, int(opaque(uint32_t(xp))), int(opaque(uint32_t(y))), int(opaque(uint32_t(z))));
     const uint32_t ps = opaque(pstride);
@@ -619,8 +745,55 @@ aa_step_paired_kernel(S* __restrict__ pops_scalar, const Geometry g, const uint8
       }
     });
   });
+}
+
+template <int Q, class S, int KIND, bool ODD, bool STATS, int CPT, int MINB>
+__global__ void __launch_bounds__(kStepThreads, MINB)
+aa_step_paired_kernel(S* __restrict__ pops, const Geometry g, const DynDevice<float> bulk,
+                      StatPartial* __restrict__ partials)
+{
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
+  const int xp = blockIdx.z;
+  const int none[CPT] = {};
+  StatAcc acc;
+  paired_tile<Q, S, KIND, ODD, false, STATS, CPT>(pops, g, nullptr, bulk, xp, y0, z, int(blockDim.y), none, none,
+                                                 acc);
   if constexpr (STATS) {
-    block_stats(s_rho, s_usqr, s_max, s_n, s_nf, partials);
+    block_stats(acc.rho, acc.usqr, acc.max, acc.n, acc.nf, partials);
+  }
+}
+
+// the masked paired kernel: persistent, ids one tile ahead (aa_step_masked_kernel)
+template <int Q, class S, int KIND, bool ODD, bool STATS, int CPT, int MINB>
+__global__ void __launch_bounds__(kStepThreads, MINB)
+aa_step_masked_paired_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict__ ids,
+                             const DynDevice<float>* __restrict__ table, const DynDevice<float> bulk,
+                             StatPartial* __restrict__ partials)
+{
+  const int nxh = g.nx >> 1;
+  const TileGrid tg(g, CPT, nxh);
+  const int dy = int(blockDim.y);
+  StatAcc acc;
+  int next_lo[CPT], next_hi[CPT];
+  auto fetch = [&](uint32_t t) {
+    int xp, y0, z;
+    tg.origin(t, xp, y0, z);
+    load_tile_ids(next_lo, g, ids, xp, y0, z, dy);
+    load_tile_ids(next_hi, g, ids, xp + nxh, y0, z, dy);
+  };
+  uint32_t t = blockIdx.x;
+  if (t < tg.tiles) fetch(t);
+  for (; t < tg.tiles; t += gridDim.x) {
+    int lo[CPT], hi[CPT];
+    static_for<0, CPT>([&](auto k) { lo[k] = next_lo[k]; hi[k] = next_hi[k]; });
+    if (t + gridDim.x < tg.tiles) fetch(t + gridDim.x);
+    int xp, y0, z;
+    tg.origin(t, xp, y0, z);
+    paired_tile<Q, S, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, xp, y0, z, dy, lo, hi, acc);
+  }
+  if constexpr (STATS) {
+    block_stats(acc.rho, acc.usqr, acc.max, acc.n, acc.nf, partials);
   }
 }
 
@@ -684,6 +857,23 @@ __global__ void scatter_natural_kernel(S* __restrict__ pops, const Geometry g,
   });
 }
 
+// FORCE of cell n of a Guo-forced dynamics: the lattice's force field when it
+// has one, else the entry's constant
+template <class R>
+OLB_DEV void cell_force(const Geometry& g, const DynDevice<R>* e, uint32_t n, R (&gg)[3])
+{
+  if (g.force) {
+    const R* F = static_cast<const R*>(g.force);
+    gg[0] = F[n];
+    gg[1] = F[size_t(g.stride) + n];
+    gg[2] = F[2 * size_t(g.stride) + n];
+  } else {
+    gg[0] = e->force[0];
+    gg[1] = e->force[1];
+    gg[2] = e->force[2];
+  }
+}
+
 // Density / velocity as the reference's Density3D / Velocity3D report them
 // (per-dynamics momenta: src/dynamics/momenta/elements.h).
 template <int Q, class S, class R>
@@ -706,7 +896,8 @@ __global__ void moments_kernel(const S* __restrict__ pops, const Geometry g, boo
     R f[Q];
     static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted); });
     if (kind == K_FORCED_BGK || kind == K_FORCED_TRT) {
-      const R gg[3] = {p->force[0], p->force[1], p->force[2]};
+      R gg[3];
+      cell_force(g, p, n, gg);
       compute_rho_u_forced<L>(f, gg, rho, u);
     } else {
       compute_rho_u<L>(f, rho, u);
@@ -802,7 +993,8 @@ OLB_DEV void cell_velocity(const S* __restrict__ pops, const Geometry& g, bool s
     static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, p[0], p[1], p[2], shifted); });
     R rho;
     if (kind == K_FORCED_BGK || kind == K_FORCED_TRT) {
-      const R gg[3] = {e->force[0], e->force[1], e->force[2]};
+      R gg[3];
+      cell_force(g, e, n, gg);
       compute_rho_u_forced<L>(f, gg, rho, u);
     } else {
       compute_rho_u<L>(f, rho, u);
@@ -1088,6 +1280,7 @@ struct StepLaunch {
   StatPartial* partials;   // device, gridDim product entries
   int block_z, block_y;
   int variant;             // index into kStepVariants
+  int sm_count;            // multiprocessors of the device (masked_grid)
   cudaStream_t stream;
 };
 
@@ -1125,6 +1318,17 @@ inline dim3 step_grid(const Geometry& g, int bz, int by, int cells_per_thread)
 {
   const int rows = by * cells_per_thread;
   return dim3((g.nz + bz - 1) / bz, (g.ny + rows - 1) / rows, g.paired ? g.nx / 2 : g.nx);
+}
+
+// Grid of the persistent masked kernels: as many blocks as are resident at
+// once — min_blocks per multiprocessor, which __launch_bounds__ guarantees —
+// and no more than there are tiles.
+inline unsigned masked_grid(const Geometry& g, int bz, int by, int cells_per_thread, int min_blocks, int sm_count)
+{
+  const dim3 grid = step_grid(g, bz, by, cells_per_thread);
+  const size_t tiles = size_t(grid.x) * grid.y * grid.z;
+  const size_t resident = size_t(sm_count > 0 ? sm_count : 1) * size_t(min_blocks);
+  return unsigned(tiles < resident ? tiles : resident);
 }
 
 // grid of the gather / moments kernels (one cell per thread)

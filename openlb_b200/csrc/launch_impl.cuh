@@ -14,37 +14,50 @@ template <int Q, class S, class R, int KIND, int CPT, int MINB>
 static cudaError_t launch_step_variant(const StepLaunch& a, bool odd, bool masked, bool stats)
 {
   const dim3 block(a.block_z, a.block_y);
-  const dim3 grid = step_grid(a.g, a.block_z, a.block_y, CPT);
   S* pops = static_cast<S*>(a.pops);
   const DynDevice<R>* table = static_cast<const DynDevice<R>*>(a.table);
   const DynDevice<R>& bulk = *static_cast<const DynDevice<R>*>(a.bulk);
   constexpr bool kHalf = std::is_same_v<S, __half> || std::is_same_v<S, __nv_bfloat16>;
-#define OLB_LAUNCH(O, M, ST)                                                                       \
+  if (masked) {
+    const dim3 grid(masked_grid(a.g, a.block_z, a.block_y, CPT, MINB, a.sm_count));
+#define OLB_LAUNCH(O, ST)                                                                          \
   do {                                                                                             \
     if constexpr (kHalf) {                                                                         \
       if (a.g.paired) {                                                                            \
-        aa_step_paired_kernel<Q, S, KIND, O, M, ST, CPT, MINB><<<grid, block, 0, a.stream>>>(      \
+        aa_step_masked_paired_kernel<Q, S, KIND, O, ST, CPT, MINB><<<grid, block, 0, a.stream>>>(  \
           pops, a.g, a.ids, table, bulk, a.partials);                                              \
         break;                                                                                     \
       }                                                                                            \
     }                                                                                              \
-    aa_step_kernel<Q, S, R, KIND, O, M, ST, CPT, MINB><<<grid, block, 0, a.stream>>>(              \
+    aa_step_masked_kernel<Q, S, R, KIND, O, ST, CPT, MINB><<<grid, block, 0, a.stream>>>(          \
       pops, a.g, a.ids, table, bulk, a.partials);                                                  \
   } while (0)
-  if (odd) {
-    if (masked) {
-      if (stats) OLB_LAUNCH(true, true, true); else OLB_LAUNCH(true, true, false);
+    if (odd) {
+      if (stats) OLB_LAUNCH(true, true); else OLB_LAUNCH(true, false);
     } else {
-      if (stats) OLB_LAUNCH(true, false, true); else OLB_LAUNCH(true, false, false);
+      if (stats) OLB_LAUNCH(false, true); else OLB_LAUNCH(false, false);
     }
-  } else {
-    if (masked) {
-      if (stats) OLB_LAUNCH(false, true, true); else OLB_LAUNCH(false, true, false);
-    } else {
-      if (stats) OLB_LAUNCH(false, false, true); else OLB_LAUNCH(false, false, false);
-    }
-  }
 #undef OLB_LAUNCH
+  } else {
+    const dim3 grid = step_grid(a.g, a.block_z, a.block_y, CPT);
+#define OLB_LAUNCH(O, ST)                                                                          \
+  do {                                                                                             \
+    if constexpr (kHalf) {                                                                         \
+      if (a.g.paired) {                                                                            \
+        aa_step_paired_kernel<Q, S, KIND, O, ST, CPT, MINB><<<grid, block, 0, a.stream>>>(         \
+          pops, a.g, bulk, a.partials);                                                            \
+        break;                                                                                     \
+      }                                                                                            \
+    }                                                                                              \
+    aa_step_kernel<Q, S, R, KIND, O, ST, CPT, MINB><<<grid, block, 0, a.stream>>>(pops, a.g, bulk, a.partials); \
+  } while (0)
+    if (odd) {
+      if (stats) OLB_LAUNCH(true, true); else OLB_LAUNCH(true, false);
+    } else {
+      if (stats) OLB_LAUNCH(false, true); else OLB_LAUNCH(false, false);
+    }
+#undef OLB_LAUNCH
+  }
   return cudaGetLastError();
 }
 

@@ -264,6 +264,8 @@ struct olb_b200_lattice {
   StatPartial* stat_host = nullptr;  // pinned
   int block_z = 0, block_y = 0;
   int variant = 0;          // index into kStepVariants
+  int sm_count = 0;         // multiprocessors of the device (grid of the masked kernels)
+  void* force = nullptr;    // FORCE per cell, 3 columns of `stride` R (olb_b200_set_force_field)
   bool tuned = false;       // variant and shape chosen by olb_b200_autotune
   float tuned_ms = 0.f;
   cudaStream_t stream = nullptr;
@@ -354,6 +356,10 @@ size_t boundary_blocks(const olb_b200_lattice* L)
 
 size_t step_blocks(const olb_b200_lattice* L)
 {
+  if (L->masked) {
+    return masked_grid(L->g, L->block_z, L->block_y, cells_per_thread(L), kStepVariants[L->variant].min_blocks,
+                       L->sm_count);
+  }
   const dim3 grid = step_grid(L->g, L->block_z, L->block_y, cells_per_thread(L));
   return size_t(grid.x) * grid.y * grid.z;
 }
@@ -368,6 +374,7 @@ void compute_bulk_box(olb_b200_lattice* L, const uint8_t* ids, int bulk_entry)
 {
   Geometry& g = L->g;
   for (int d = 0; d < 3; ++d) g.bulk_lo[d] = g.bulk_hi[d] = 0;
+  g.bulk_id = bulk_entry < 0 ? 0 : bulk_entry;
   if (!ids || bulk_entry < 0) return;
   const int n[3] = {L->desc.nx, L->desc.ny, L->desc.nz};
   auto id_at = [&](int x, int y, int z) { return int(ids[(size_t(x) * n[1] + y) * n[2] + z]); };
@@ -465,6 +472,7 @@ olb_b200_status enqueue_steps(olb_b200_lattice* L, int steps, bool stats_last)
     a.block_z = L->block_z;
     a.block_y = L->block_y;
     a.variant = L->variant;
+    a.sm_count = L->sm_count;
     a.stream = L->stream;
     const bool odd = L->parity == 1;
     cudaError_t e = cudaSuccess;
@@ -503,6 +511,7 @@ olb_b200_status setup_boundaries(olb_b200_lattice* L, const uint8_t* ids, const 
   if (L->bc_values) cudaFree(L->bc_values);
   if (L->bc_u) cudaFree(L->bc_u);
   if (L->bc_base) cudaFree(L->bc_base);
+  if (L->force) cudaFree(L->force);
   L->bc_base = nullptr;
   L->bc_cells = nullptr;
   L->bc_values = nullptr;
@@ -696,6 +705,7 @@ olb_b200_status olb_b200_create(const olb_b200_desc* desc, olb_b200_lattice** ou
     cudaError_t e_ = (call);                                                                       \
     if (e_ != cudaSuccess) return cleanup(cuda_fail(e_, #call));                                   \
   } while (0)
+  OLB_CUDA_C(cudaDeviceGetAttribute(&L->sm_count, cudaDevAttrMultiProcessorCount, L->device));
   OLB_CUDA_C(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
   OLB_CUDA_C(cudaEventCreate(&L->ev0));
   OLB_CUDA_C(cudaEventCreate(&L->ev1));
@@ -736,6 +746,7 @@ void olb_b200_destroy(olb_b200_lattice* L)
   if (L->bc_values) cudaFree(L->bc_values);
   if (L->bc_u) cudaFree(L->bc_u);
   if (L->bc_base) cudaFree(L->bc_base);
+  if (L->force) cudaFree(L->force);
   if (L->stat_dev) cudaFree(L->stat_dev);
   if (L->stat_host) cudaFreeHost(L->stat_host);
   if (L->ev0) cudaEventDestroy(L->ev0);
@@ -1146,6 +1157,43 @@ olb_b200_status olb_b200_set_boundary_values(olb_b200_lattice* L, const int64_t*
   }
   OLB_CUDA(cudaStreamSynchronize(L->stream));
   return upload_boundary_values(L);
+}
+
+olb_b200_status olb_b200_set_force_field(olb_b200_lattice* L, const void* force)
+{
+  g_last_error.clear();
+  if (!L) return fail(OLB_B200_ERR_ARG, "set_force_field: null lattice");
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  const size_t column = L->stride * L->real;  // bytes per component column
+  if (!force) {
+    if (L->force) {
+      cudaFree(L->force);
+      L->device_bytes -= 3 * column;
+    }
+    L->force = nullptr;
+    L->g.force = nullptr;
+    return OLB_B200_OK;
+  }
+  if (!L->force) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, 3 * column);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      return fail(OLB_B200_ERR_OOM, "set_force_field: cudaMalloc(%zu) failed", 3 * column);
+    }
+    L->force = p;
+    L->device_bytes += 3 * column;
+    OLB_CUDA(cudaMemset(L->force, 0, 3 * column));
+  }
+  for (int d = 0; d < 3; ++d) {
+    OLB_CUDA(cudaMemcpy(static_cast<char*>(L->force) + d * column,
+                        static_cast<const char*>(force) + d * L->cells * L->real, L->cells * L->real,
+                        cudaMemcpyHostToDevice));
+  }
+  L->g.force = L->force;
+  return OLB_B200_OK;
 }
 
 olb_b200_status olb_b200_set_boundary_noise(olb_b200_lattice* L, double amplitude, uint64_t seed)

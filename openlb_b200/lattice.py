@@ -231,6 +231,17 @@ class Lattice:
         self._check(self._lib.olb_b200_set_boundary_values(self._h, cells.ctypes.data, cells.size,
                                                            values.ctypes.data))
 
+    def set_force_field(self, force: np.ndarray | None) -> None:
+        """A FORCE value per cell for the Guo-forced dynamics (``force`` of
+        shape (3, cells) or (3, nx, ny, nz), the cells in population order), in
+        place of their entries' constant force; None removes it
+        (olb_b200_set_force_field)."""
+        if force is None:
+            self._check(self._lib.olb_b200_set_force_field(self._h, None))
+            return
+        f = np.ascontiguousarray(np.asarray(force).reshape(3, self.n), dtype=self.dtype)
+        self._check(self._lib.olb_b200_set_force_field(self._h, f.ctypes.data))
+
     def set_boundary_noise(self, amplitude: float, seed: int = 0) -> None:
         """Per-step inlet fluctuations of relative size ``amplitude`` (see
         olb_b200_set_boundary_noise; :func:`inlet_noise` computes the same
@@ -415,6 +426,7 @@ class SuperLattice:
         self._dyn_of_material: dict[int, Dynamics] = {}
         self._params = {"OMEGA": None}
         self._force: dict[int, tuple] = {}
+        self._force_field = None                  # (3, n): FORCE per cell, once a field was defined
         self._wall_u: dict[int, tuple] = {}
         self._wall_rho: dict[int, float] = {}
         self._pending_pops = np.zeros((self.descriptor.q, self.block.n), self.block.dtype)
@@ -451,9 +463,25 @@ class SuperLattice:
     def setParameter(self, name: str, value: float) -> None:
         self._params[name] = float(value)
 
-    # defineField<FORCE>(superGeometry, material, value)
+    # defineField<FORCE>(superGeometry, material, value): a constant 3-vector,
+    # or a (3, nx, ny, nz) field whose values the material's cells take
     def defineForce(self, geometry: SuperGeometry, material: int, force) -> None:
-        self._force[int(material)] = tuple(float(f) for f in force)
+        m = int(material)
+        fa = np.asarray(force, dtype=np.float64)
+        if fa.size == 3 and self._force_field is None:
+            self._force[m] = tuple(float(f) for f in fa.reshape(3))
+            return
+        if self._force_field is None:
+            # from now on every forced cell reads the field: seed it with the
+            # constants defined so far
+            self._force_field = np.zeros((3, self.block.n))
+            flat = self.geometry.materials.reshape(-1)
+            for mm, g in self._force.items():
+                self._force_field[:, flat == mm] = np.asarray(g, np.float64)[:, None]
+        cells = self._bc_cells(m)
+        self._force_field[:, cells] = fa.reshape(3, 1) if fa.size == 3 else fa.reshape(3, -1)[:, cells]
+        if self._initialized:
+            self.block.set_force_field(self._force_field)
 
     # defineU(superGeometry, material, u): the VELOCITY field of moving walls,
     # or per cell on interpolated boundaries (u: a 3-vector or a (3, nx, ny, nz) field)
@@ -523,6 +551,8 @@ class SuperLattice:
     def initialize(self) -> None:
         table, ids = self._table()
         self.block.set_dynamics(table, ids)
+        if self._force_field is not None:
+            self.block.set_force_field(self._force_field)
         self._initialized = True
         for m in self._bc:
             self._push_values(m)
@@ -580,8 +610,11 @@ class SuperLattice:
         inlet fluctuations on, those are the base values)."""
         from . import checkpoint as CK
         table, ids = self._table()
-        return CK.setup_fields(self.descriptor.q, ids, table, descriptor_fields,
-                               bc_values=self._values() if self._bc else None)
+        fields, values = CK.setup_fields(self.descriptor.q, ids, table, descriptor_fields,
+                                         bc_values=self._values() if self._bc else None)
+        if self._force_field is not None and "FORCE" in values:
+            values["FORCE"] = self._force_field.astype(values["FORCE"].dtype).reshape(values["FORCE"].shape)
+        return fields, values
 
     # Serializable::save(fileName) (core/serializer.hh:145-149), without the
     # log-directory prefix: writes <fileName>_rank0_size1.dat

@@ -355,6 +355,9 @@ private:
   std::vector<olb_b200_dyn_params> _table;
   std::vector<std::int64_t> _valueCells;  // boundary cells with values, logical index
   std::vector<double> _values;            // 4 per cell: RHO, VELOCITY x, y, z
+  /// FORCE per cell (x of every cell, then y, then z) when the Guo-forced
+  /// cells do not all share one value; empty: the entries carry the force
+  std::vector<T> _forceField;
 
   void buildTable()
   {
@@ -382,6 +385,12 @@ private:
     std::size_t n = 0;
     _valueCells.clear();
     _values.clear();
+    // FORCE of the forced cells, gathered while their entries are keyed
+    // without it (one entry per forced dynamics and parameter set)
+    std::vector<double> force;
+    bool anyForced = false, uniformForce = true;
+    double firstForce[3] = {0., 0., 0.};
+    const std::size_t cells = std::size_t(nx) * ny * nz;
     for (int iX = 0; iX < nx; ++iX) {
       for (int iY = 0; iY < ny; ++iY) {
         for (int iZ = 0; iZ < nz; ++iZ, ++n) {
@@ -419,6 +428,20 @@ private:
               p.normal[iD] = it->second[1 + iD];
             }
           }
+          if (p.kind == OLB_B200_DYN_FORCED_BGK || p.kind == OLB_B200_DYN_FORCED_TRT) {
+            if (force.empty()) {
+              force.assign(3 * cells, 0.);
+            }
+            for (int iD = 0; iD < 3; ++iD) {
+              force[iD * cells + n] = p.force[iD];
+              if (!anyForced) {
+                firstForce[iD] = p.force[iD];
+              }
+              uniformForce = uniformForce && p.force[iD] == firstForce[iD];
+              p.force[iD] = 0.;
+            }
+            anyForced = true;
+          }
           if (lastOp->valued()) {
             double v[4];
             lastOp->values(*_block, iCell, v);
@@ -447,6 +470,19 @@ private:
         }
       }
     }
+    _forceField.clear();
+    if (anyForced && uniformForce) {
+      // one value everywhere: it goes back into the entries
+      for (auto& e : table) {
+        if (e.kind == OLB_B200_DYN_FORCED_BGK || e.kind == OLB_B200_DYN_FORCED_TRT) {
+          for (int iD = 0; iD < 3; ++iD) {
+            e.force[iD] = firstForce[iD];
+          }
+        }
+      }
+    } else if (anyForced) {
+      _forceField.assign(force.begin(), force.end());
+    }
     _ids = std::move(ids);
     _table = std::move(table);
     _epochAtUpload = dynamicsEpoch().load(std::memory_order_relaxed);
@@ -460,6 +496,8 @@ private:
     }
     check(olb_b200_set_dynamics(_handle, needIds ? _ids.data() : nullptr, _table.data(),
                                 int32_t(_table.size())), "set_dynamics");
+    check(olb_b200_set_force_field(_handle, _forceField.empty() ? nullptr : _forceField.data()),
+          "set_force_field");
     if (!_valueCells.empty()) {
       check(olb_b200_set_boundary_values(_handle, _valueCells.data(), std::int64_t(_valueCells.size()),
                                          _values.data()), "set_boundary_values");

@@ -21,7 +21,7 @@ import numpy as np
 from . import _abi
 from .lattice import (BGKdynamics, BounceBack, BounceBackVelocity, ForcedTRTdynamics, Lattice,
                       SmagorinskyBGKdynamics)
-from .workloads import cavity
+from .workloads import cavity, porous_spheres
 
 BYTES = {"f32": 4, "f64": 8, "f16": 2, "bf16": 2}
 CLASSES = [
@@ -55,6 +55,15 @@ def peak_gbs() -> float:
         return 6650.0
 
 
+def make_porous(size, storage, q=19):
+    """The porous channel: x-periodic, bounce-back y/z walls and spheres of
+    radius U[6,14] up to 35 % solid, forced TRT (tau 0.8, magic 3/16, g 1e-6)."""
+    ids, _, _ = porous_spheres(size, seed=3)
+    lat = Lattice(q, size, (True, False, False), storage=storage)
+    lat.set_dynamics([ForcedTRTdynamics(omega=1 / 0.8, magic=3 / 16, force=(1e-6, 0.0, 0.0)), BounceBack()], ids)
+    return lat
+
+
 def make_lattice(q, n, storage, masked, collision="bgk"):
     lat = Lattice(q, (n, n, n), (not masked,) * 3, storage=storage)
     if masked:
@@ -72,21 +81,32 @@ def time_config(lat, steps, repeat):
 
 
 def run_single(args):
-    """One fixed configuration: warm-up, then `--steps` steps (for profilers)."""
-    lat = make_lattice(args.lattice, args.n, args.storage, args.masked)
+    """Fixed configurations: for each variant of `--variant` (comma-separated)
+    and each launch shape of `--shape` (';'-separated), warm-up, then
+    `--steps` steps (for profilers; one JSON line each)."""
+    if args.porous:
+        size = tuple(int(v) for v in args.porous.split(","))
+        lat = make_porous(size, args.storage, args.lattice)
+    else:
+        size = (args.n,) * 3
+        lat = make_lattice(args.lattice, args.n, args.storage, args.masked)
+    cells = int(np.prod(size))
+    bpc = 2 * args.lattice * BYTES[args.storage]
     try:
-        lat.set_step_variant(args.variant)
-        bz, by = (int(v) for v in args.shape.split(","))
-        lat.set_launch_shape(bz, by)
-        lat.collide_and_stream(args.warmup)
-        lat.synchronize()
-        ms = lat.time_steps(args.steps)
-        cells = args.n ** 3
-        bpc = 2 * args.lattice * BYTES[args.storage]
-        print(json.dumps({"lattice": args.lattice, "n": args.n, "storage": args.storage, "masked": args.masked,
-                          "tuning": lat.tuning(), "ms_per_step": ms / args.steps,
-                          "mlups": round(cells * args.steps / (ms * 1e-3) / 1e6),
-                          "frac": round(cells * bpc * args.steps / (ms * 1e-3) / 1e9 / peak_gbs(), 3)}))
+        for variant in (int(v) for v in str(args.variant).split(",")):
+            for shape in args.shape.split(";"):
+                lat.set_step_variant(variant)
+                bz, by = (int(v) for v in shape.split(","))
+                lat.set_launch_shape(bz, by)
+                lat.collide_and_stream(args.warmup)
+                lat.synchronize()
+                ms = lat.time_steps(args.steps)
+                print(json.dumps({"lattice": args.lattice, "size": list(size), "storage": args.storage,
+                                  "workload": "porous" if args.porous else ("cavity" if args.masked else "periodic"),
+                                  "tuning": lat.tuning(), "ms_per_step": ms / args.steps,
+                                  "mlups": round(cells * args.steps / (ms * 1e-3) / 1e6),
+                                  "frac": round(cells * bpc * args.steps / (ms * 1e-3) / 1e9 / peak_gbs(), 3)}),
+                      flush=True)
     finally:
         lat.close()
 
@@ -100,9 +120,11 @@ def main(argv=None):
                     help="run one fixed configuration (--lattice/--storage/--masked/--variant/--shape)")
     ap.add_argument("--lattice", type=int, default=19, choices=[19, 27])
     ap.add_argument("--storage", default="f32", choices=list(BYTES))
-    ap.add_argument("--masked", action="store_true")
-    ap.add_argument("--variant", type=int, default=-1)
-    ap.add_argument("--shape", default="128,2")
+    ap.add_argument("--masked", action="store_true", help="lid-driven cavity (walls and a moving lid)")
+    ap.add_argument("--porous", default="", metavar="NX,NY,NZ",
+                    help="--single: the porous channel of this size instead of a cube")
+    ap.add_argument("--variant", default="-1", help="--single: variant(s), comma-separated (-1: default)")
+    ap.add_argument("--shape", default="128,2", help="--single: launch shape(s) bz,by; ';'-separated")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--classes", default="", help="';'-separated substrings of the class labels to run")
     args = ap.parse_args(argv)

@@ -75,6 +75,10 @@ typedef struct {
   /* boundary values of interpolated cells, [4][cells]: RHO (fixed density of
    * pressure cells), then the VELOCITY field x, y, z; NULL if none */
   const double* bc_values;
+  /* the FORCE field per cell, [3][cells], read by the Guo-forced dynamics in
+   * place of their entry's force (forcing::Guo, dynamics/forcing.h:53-69,
+   * momenta::ForcedMomentum, momenta/elements.h:1480-1488); NULL: the entry's */
+  const double* force_field;
 } oracle_lattice;
 
 typedef struct {

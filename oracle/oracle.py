@@ -55,6 +55,7 @@ class _Lattice(ctypes.Structure):
         ("nz", ctypes.c_int32), ("periodic", ctypes.c_int32 * 3), ("n_dyn", ctypes.c_int32),
         ("dyn_id", ctypes.c_void_p), ("table", ctypes.POINTER(_Dyn)),
         ("bc_values", ctypes.c_void_p),
+        ("force_field", ctypes.c_void_p),
     ]
 
 
@@ -91,6 +92,7 @@ class Case:
     dyn_id: np.ndarray | None = None  # uint8[nx*ny*nz]
     extra: dict = field(default_factory=dict)
     bc_values: np.ndarray | None = None  # float64[4][nx*ny*nz]: RHO, VELOCITY x, y, z
+    force_field: np.ndarray | None = None  # float64[3][nx*ny*nz]: FORCE per cell (forced dynamics)
 
     @property
     def n(self) -> int:
@@ -151,6 +153,13 @@ def _lattice(case: Case, keep: list):
         lat.bc_values = v.ctypes.data
     else:
         lat.bc_values = None
+    if case.force_field is not None:
+        ff = np.ascontiguousarray(case.force_field, dtype=np.float64)
+        assert ff.size == 3 * case.n
+        keep.append(ff)
+        lat.force_field = ff.ctypes.data
+    else:
+        lat.force_field = None
     return lat
 
 
@@ -288,6 +297,10 @@ def write_case(dirpath: Path, case: Case, steps: int, init: np.ndarray | None = 
         dt = init.dtype if init is not None else rhou.dtype
         np.ascontiguousarray(vals, dtype=dt).tofile(dirpath / "bcvalues.bin")
         lines.append("bcvalues 1")
+    if case.force_field is not None:
+        dt = init.dtype if init is not None else rhou.dtype
+        np.ascontiguousarray(case.force_field, dtype=dt).tofile(dirpath / "forcefield.bin")
+        lines.append("forcefield 1")
     if normals:
         lines.append(f"normals {int(normals)}")
     if init is not None:

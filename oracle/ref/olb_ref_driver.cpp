@@ -87,6 +87,7 @@ struct Case {
   int benchWarmup = -1, benchSteps = 0;
   std::string bcMixin = "bgk";
   bool bcValues = false;
+  bool forceField = false;                    // FORCE per cell from forcefield.bin
   int dumpNormals = 0;
   std::string loadPath, savePath;             // checkpoints (Serializable), relative to the case dir
 };
@@ -119,6 +120,7 @@ Case parse_case(const std::string& dir)
     else if (key == "bench") { ls >> c.benchWarmup >> c.benchSteps; }
     else if (key == "bcmixin") { ls >> c.bcMixin; }
     else if (key == "bcvalues") { int b; ls >> b; c.bcValues = b; }
+    else if (key == "forcefield") { int b; ls >> b; c.forceField = b; }
     else if (key == "normals") { ls >> c.dumpNormals; }
     else if (key == "load") { ls >> c.loadPath; }
     else if (key == "save") { ls >> c.savePath; }
@@ -271,6 +273,20 @@ int main(int argc, char* argv[])
   for (auto& [m, g] : cs.force) {
     AnalyticalConst3D<T,T> forceF(std::vector<T>{T(g[0]), T(g[1]), T(g[2])});
     lattice.template defineField<descriptors::FORCE>(geometry, m, forceF);
+  }
+  // a FORCE value per cell (every cell; only the forced dynamics read it)
+  if (cs.forceField) {
+    auto force = read_array<T>(dir + "/forcefield.bin", 3 * n);
+    auto& block = lattice.getBlock(0);
+    for (int x = 0; x < nx; ++x) {
+      for (int y = 0; y < ny; ++y) {
+        for (int z = 0; z < nz; ++z) {
+          const std::size_t i = (std::size_t(x) * ny + y) * nz + z;
+          auto cell = block.get({x, y, z});
+          cell.template setField<descriptors::FORCE>(Vector<T,3>{force[i], force[n + i], force[2 * n + i]});
+        }
+      }
+    }
   }
 
   // Initial populations: either given directly, or the equilibrium of given

@@ -82,6 +82,18 @@ def porous_case(q, size, rng, omega=1.2, magic=3 / 16, g=1e-5):
                          O.Dynamics(O.BOUNCE_BACK)])
 
 
+def with_force_field(case, dtype, rng, g=1e-4, spread=0.5):
+    """The case with a FORCE value per cell: x component g (1 + spread U[-1,1]),
+    y and z g spread U[-1,1]/2, rounded to `dtype` (the values a lattice of that
+    precision stores), kept as float64 for the oracle."""
+    n = case.n
+    f = np.empty((3, n))
+    f[0] = g * (1 + spread * rng.uniform(-1, 1, n))
+    f[1:] = 0.5 * g * spread * rng.uniform(-1, 1, (2, n))
+    case.force_field = f.astype(dtype).astype(np.float64)
+    return case
+
+
 def channel_cylinder_case(q, size, omega=1.6, smagorinsky=0.1, side=4):
     """x-periodic channel (bounce-back y/z walls) with a square cylinder
     spanning z; Smagorinsky BGK fluid."""

@@ -95,6 +95,19 @@ def fixture_cases():
         for variant in (("sisd", "nocse") if (q == 19 and dtype == np.float32) else ("sisd",)):
             name = f"open_inlet_q{q}_{np.dtype(dtype).name}_{O.KIND_NAMES[mixin]}_{variant}"
             out.append((name, case, f0, 15, dtype, variant, True))
+    # a FORCE value per cell (setField<FORCE> cell by cell) for the Guo-forced
+    # dynamics: porous channel with forced TRT, periodic D3Q27 forced BGK
+    frng = np.random.default_rng(31)
+    for q, dtype, variants in ((19, np.float32, ("sisd", "nocse")), (19, np.float64, ("sisd",)),
+                               (27, np.float32, ("sisd",))):
+        case = C.with_force_field(C.porous_case(q, (12, 9, 8), np.random.default_rng(7), g=1e-4), dtype, frng)
+        f0 = C.rest_state(q, case.n, dtype)
+        for variant in variants:
+            out.append((f"forcefield_porous_q{q}_{np.dtype(dtype).name}_{variant}", case, f0, 15, dtype, variant,
+                        True))
+    case = C.with_force_field(C.periodic_case(27, (7, 6, 5), kind=O.FORCED_BGK), np.float64, frng)
+    f0 = C.random_state(27, case.n, np.float64, frng)
+    out.append(("forcefield_periodic_q27_float64_forced_bgk_sisd", case, f0, 4, np.float64, "sisd", True))
     return out
 
 
@@ -250,6 +263,8 @@ def main(only: str | None = None):
             payload["stats"] = ref["stats"]
         if case.bc_values is not None:
             payload["bc_values"] = case.bc_values
+        if case.force_field is not None:
+            payload["force_field"] = case.force_field
         path = HERE / f"{name}.npz"
         np.savez_compressed(path, **payload)
         manifest[name] = {"variant": variant, "dtype": np.dtype(dtype).name, "steps": steps,

@@ -1,0 +1,202 @@
+"""GPU parity of the per-cell FORCE field (olb_b200_set_force_field).
+
+OpenLB's Guo-forced dynamics read the cell's FORCE field
+(forcing::Guo, src/dynamics/forcing.h:53-69; the forced momenta add F/2 to
+the velocity, src/dynamics/momenta/elements.h:1480-1488), which an example
+sets cell by cell (defineField<FORCE>, Cell::setField).  The fixtures
+(tests/golden/forcefield_*) are OpenLB's own CPU runs with a different FORCE
+value in every cell.
+
+Tolerances, relative to the unshifted population f_i: FP32 1e-5, FP64 1e-10
+(fixtures) / 1e-12 (oracle); the exact build is bit-identical to the oracle; a
+uniform field gives the same bits as the entry's constant force; 16-bit
+storage: velocity L2 against the FP64 oracle <= 1e-3 (f16) and 5e-3 (bf16).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import openlb_b200 as ob
+from oracle import oracle as O
+from tests import cases as C
+from tests.test_oracle_golden import load
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+FIXTURES = sorted(p.stem for p in GOLDEN.glob("forcefield_*.npz"))
+
+
+def run_gpu(case, f0, steps, storage="f32", variant="fast", field=None, shape=None):
+    """``field``: the force field to set (default: the case's)."""
+    lat = ob.Lattice(case.q, case.size, case.periodic, storage=storage, variant=variant)
+    try:
+        lat.set_dynamics(C.to_abi_table(case), case.dyn_id)
+        ff = case.force_field if field is None else field
+        if ff is not None:
+            lat.set_force_field(ff)
+        if shape is not None:
+            lat.set_launch_shape(*shape)
+        lat.set_populations(f0)
+        lat.collide_and_stream(steps)
+        pops = lat.get_populations()
+        rho, u = lat.get_moments()
+        return pops, rho, u
+    finally:
+        lat.close()
+
+
+def run_oracle(case, f0, steps):
+    f = f0.copy()
+    O.step(case, f, steps)
+    return f
+
+
+def _cases(q, dtype, rng):
+    return {
+        "porous": C.with_force_field(C.porous_case(q, (16, 11, 10), np.random.default_rng(4), g=1e-4), dtype, rng),
+        "periodic_trt": C.with_force_field(C.periodic_case(q, (9, 8, 7), kind=O.FORCED_TRT), dtype, rng),
+        "periodic_bgk": C.with_force_field(C.periodic_case(q, (9, 8, 7), kind=O.FORCED_BGK), dtype, rng),
+    }
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_matches_reference_fixture(name):
+    z, case = load(name)
+    assert case.force_field is not None
+    storage = "f64" if z["init"].dtype == np.float64 else "f32"
+    steps = int(z["steps"])
+    got, rho, u = run_gpu(case, z["init"], steps, storage=storage)
+    tol = 1e-10 if storage == "f64" else 1e-5
+    ref = np.where(np.isnan(run_oracle(case, z["init"], steps)), np.nan, z["pops"])
+    rel, _ = C.pop_tolerance_violation(case.q, got, ref, tol)
+    assert rel <= tol, (name, rel)
+    keep = np.array([case.table[i].kind != O.BOUNCE_BACK for i in
+                     (case.dyn_id if case.dyn_id is not None else np.zeros(case.n, np.uint8))])
+    np.testing.assert_allclose(u[:, keep], z["u"][:, keep], rtol=0, atol=10 * tol)
+    np.testing.assert_allclose(rho[keep], z["rho"][keep], rtol=10 * tol, atol=0)
+
+
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("storage", ["f32", "f64"])
+def test_matches_oracle(q, storage):
+    dtype = np.float64 if storage == "f64" else np.float32
+    rng = np.random.default_rng(q)
+    for which, case in _cases(q, dtype, rng).items():
+        f0 = C.random_state(q, case.n, dtype, rng, amp_u=0.01, amp_neq=1e-4)
+        for steps in (1, 2, 17):
+            ref = run_oracle(case, f0, steps)
+            got, rho, u = run_gpu(case, f0, steps, storage=storage)
+            tol = 1e-12 if storage == "f64" else 1e-5
+            rel, _ = C.pop_tolerance_violation(q, got, ref, tol)
+            assert rel <= tol, (which, steps, rel)
+            r_rho, r_u = O.moments(case, np.nan_to_num(ref))
+            fluid = np.array([case.table[i].kind in (O.FORCED_BGK, O.FORCED_TRT) for i in
+                              (case.dyn_id if case.dyn_id is not None else np.zeros(case.n, np.uint8))])
+            np.testing.assert_allclose(u[:, fluid], r_u[:, fluid], rtol=0, atol=10 * tol)
+
+
+@pytest.mark.parametrize("q", [19, 27])
+@pytest.mark.parametrize("storage", ["f32", "f64"])
+def test_exact_build_is_bit_identical(q, storage):
+    dtype = np.float64 if storage == "f64" else np.float32
+    rng = np.random.default_rng(100 + q)
+    for which, case in _cases(q, dtype, rng).items():
+        f0 = C.random_state(q, case.n, dtype, rng, amp_u=0.01, amp_neq=1e-4)
+        for steps in (1, 6):
+            ref = run_oracle(case, f0, steps)
+            got, _, _ = run_gpu(case, f0, steps, storage=storage, variant="exact")
+            valid = ~np.isnan(ref)
+            assert np.array_equal(got[valid], ref[valid]), (which, steps)
+
+
+@pytest.mark.parametrize("storage", ["f32", "f64", "f16"])
+@pytest.mark.parametrize("variant", ["fast", "exact"])
+def test_uniform_field_equals_constant_force(storage, variant):
+    """A field holding the entry's force everywhere gives the same bits as no
+    field; removing the field restores the constant."""
+    dtype = np.float64 if storage == "f64" else np.float32
+    rng = np.random.default_rng(5)
+    for case in (C.porous_case(19, (16, 11, 10), np.random.default_rng(4), g=1e-4),
+                 C.periodic_case(19, (10, 8, 7), kind=O.FORCED_TRT)):
+        g = next(d.force for d in case.table if d.kind in (O.FORCED_BGK, O.FORCED_TRT))
+        uniform = np.repeat(np.asarray(g, dtype=np.float64)[:, None], case.n, axis=1)
+        f0 = C.random_state(19, case.n, dtype, rng, amp_u=0.01, amp_neq=1e-4).astype(np.float32 if storage == "f16"
+                                                                                          else dtype)
+        plain, _, u_plain = run_gpu(case, f0, 7, storage=storage, variant=variant)
+        with_field, _, u_field = run_gpu(case, f0, 7, storage=storage, variant=variant, field=uniform)
+        assert np.array_equal(plain, with_field)
+        assert np.array_equal(u_plain, u_field)
+    lat = ob.Lattice(19, (10, 8, 7), (True, True, True), storage=storage, variant=variant)
+    try:
+        case = C.periodic_case(19, (10, 8, 7), kind=O.FORCED_TRT)
+        lat.set_dynamics(C.to_abi_table(case))
+        f0 = C.rest_state(19, case.n, np.float64 if storage == "f64" else np.float32)
+        lat.set_force_field(np.full((3, case.n), 3e-4))
+        lat.set_force_field(None)
+        lat.set_populations(f0)
+        lat.collide_and_stream(5)
+        cleared = lat.get_populations()
+    finally:
+        lat.close()
+    plain, _, _ = run_gpu(case, f0, 5, storage=storage, variant=variant)
+    assert np.array_equal(cleared, plain)
+
+
+@pytest.mark.parametrize("storage,bound", [("f16", 1e-3), ("bf16", 5e-3)])
+@pytest.mark.parametrize("nx", [16, 15])
+def test_16bit_storage_velocity_error(storage, bound, nx):
+    """Paired layout (nx even) and one cell per element (nx odd)."""
+    rng = np.random.default_rng(nx)
+    case = C.with_force_field(C.porous_case(19, (nx, 12, 11), np.random.default_rng(4), g=2e-5), np.float32, rng)
+    f0 = C.rest_state(19, case.n, np.float64)
+    ref = run_oracle(case, f0, 400)
+    _, r_u = O.moments(case, np.nan_to_num(ref))
+    _, _, u = run_gpu(case, f0.astype(np.float32), 400, storage=storage)
+    fluid = case.dyn_id == 0
+    err = np.linalg.norm(u[:, fluid] - r_u[:, fluid]) / np.linalg.norm(r_u[:, fluid])
+    assert err <= bound, err
+
+
+def test_launch_shapes_and_variants_agree():
+    rng = np.random.default_rng(9)
+    case = C.with_force_field(C.porous_case(19, (12, 21, 40), np.random.default_rng(4), g=1e-4), np.float32, rng)
+    f0 = C.random_state(19, case.n, np.float32, rng, amp_u=0.01, amp_neq=1e-4)
+    ref, _, _ = run_gpu(case, f0, 5, variant="exact")
+    for variant in range(4):
+        for shape in ((256, 1), (32, 8)):
+            lat = ob.Lattice(19, case.size, case.periodic, storage="f32", variant="exact")
+            try:
+                lat.set_dynamics(C.to_abi_table(case), case.dyn_id)
+                lat.set_force_field(case.force_field)
+                lat.set_step_variant(variant)
+                lat.set_launch_shape(*shape)
+                lat.set_populations(f0)
+                lat.collide_and_stream(5)
+                assert np.array_equal(lat.get_populations(), ref), (variant, shape)
+            finally:
+                lat.close()
+
+
+def test_facade_define_force_field():
+    """SuperLattice.defineForce with a per-cell field on the fluid material."""
+    size = (12, 9, 8)
+    rng = np.random.default_rng(2)
+    case = C.with_force_field(C.porous_case(19, size, np.random.default_rng(7), g=1e-4), np.float32, rng)
+    geom = ob.SuperGeometry(size, periodic=case.periodic)
+    geom.materials[...] = case.dyn_id.reshape(size).astype(np.int32) + 1
+    sl = ob.SuperLattice(geom, "D3Q19", storage="f32")
+    fluid = case.table[0]
+    sl.defineDynamics(geom, 1, ob.ForcedTRTdynamics(omega=fluid.omega, magic=fluid.magic))
+    sl.defineDynamics(geom, 2, ob.BounceBack())
+    sl.defineForce(geom, 1, case.force_field.reshape((3,) + size))
+    sl.iniEquilibrium(geom, 1, 1.0, (0.0, 0.0, 0.0))
+    sl.iniEquilibrium(geom, 2, 1.0, (0.0, 0.0, 0.0))
+    sl.collideAndStream(9)
+    got = sl.getPopulations().reshape(-1)
+    sl.block.close()
+    f0 = C.rest_state(19, case.n, np.float32)
+    ref = run_oracle(case, f0, 9)
+    rel, _ = C.pop_tolerance_violation(19, got, ref, 1e-5)
+    assert rel <= 1e-5

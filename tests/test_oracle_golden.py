@@ -42,7 +42,8 @@ def load(name):
                         boundary=int(r[17]) if len(r) > 17 else O.LOCAL_VELOCITY) for r in z["table"]]
     case = O.Case(q=int(z["q"]), size=tuple(int(s) for s in z["size"]),
                   periodic=tuple(int(p) for p in z["periodic"]), table=table, dyn_id=z["dyn_id"],
-                  bc_values=z["bc_values"] if "bc_values" in z.files else None)
+                  bc_values=z["bc_values"] if "bc_values" in z.files else None,
+                  force_field=z["force_field"] if "force_field" in z.files else None)
     return z, case
 
 
