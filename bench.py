@@ -333,7 +333,7 @@ def run_serve(args, world, rank, local):
     own line with the total solves/s of all ranks as value."""
     from openlb_b200 import serving
     reqs = serving.make_requests(args.requests, args.rate, SERVE["seed"] + rank, SERVE["sides"], SERVE["re"],
-                                 SERVE["lid"], SERVE["tol"], args.max_steps)
+                                 SERVE["lid"], SERVE["tol"], args.max_steps, tables=True)
     b = serving.serve_batched(reqs, int(args.budget_gb * 2 ** 30), 4096, SERVE["check"], device=local)
     steps = {r.rid: r.steps for r in b["results"]}
     cell_steps = float(sum(r.cells * steps[r.rid] for r in reqs))
@@ -418,7 +418,8 @@ def main_serve(args, world, rank, local):
     config = {"workload": SERVE["name"], "requests": args.requests, "sides": list(SERVE["sides"]),
               "re_log_uniform": list(SERVE["re"]), "lid": list(SERVE["lid"]), "tol": SERVE["tol"],
               "max_steps": args.max_steps, "budget_gb": args.budget_gb, "arrivals": f"poisson {args.rate}/s",
-              "seed": SERVE["seed"], "check_interval": SERVE["check"], "lattice": "D3Q19", "collision": "BGK",
+              "seed": SERVE["seed"], "check_interval": SERVE["check"], "geometry": "per-instance tables",
+              "lattice": "D3Q19", "collision": "BGK",
               "storage": "f32", "parallelism": f"replicas{world}" if world > 1 else "single-gpu"}
     line = {"metric": "solves/s", "unit": "solves/s", "n_gpus": world, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "data": "synthetic", "dtype": "f32", "config": config}

@@ -339,8 +339,12 @@ typedef struct olb_b200_ensemble olb_b200_ensemble;
 typedef enum {
   OLB_B200_ENSEMBLE_CAVITY = 1,   /* lid-driven cavity: bounce-back box, lid wall_u on y = ny-1,
                                      BGK fluid (cavity3dBenchmark geometry) */
-  OLB_B200_ENSEMBLE_CHANNEL = 2   /* x-periodic channel, bounce-back walls at y and z faces,
+  OLB_B200_ENSEMBLE_CHANNEL = 2,  /* x-periodic channel, bounce-back walls at y and z faces,
                                      Guo-forced BGK fluid with body force `force` */
+  OLB_B200_ENSEMBLE_GEOMETRY = 3  /* the instance's own geometry table `cells`: one byte per
+                                     cell (z fastest), 0 fluid, 1 bounce-back wall, 2 moving wall
+                                     with velocity wall_u; BGK fluid, Guo-forced BGK when `force`
+                                     is nonzero; every axis wraps (a face is closed by wall cells) */
 } olb_b200_instance_kind;
 
 typedef struct {
@@ -355,8 +359,10 @@ typedef struct {
   int32_t kind;           /* olb_b200_instance_kind */
   int32_t nx, ny, nz;
   double omega;
-  double wall_u[3];       /* lid velocity (cavity) */
-  double force[3];        /* body force (channel) */
+  double wall_u[3];       /* lid velocity (cavity), moving-wall velocity (geometry) */
+  double force[3];        /* body force (channel, geometry) */
+  const uint8_t* cells;   /* OLB_B200_ENSEMBLE_GEOMETRY: nx*ny*nz cell classes, copied by
+                             olb_b200_ensemble_add; NULL otherwise */
 } olb_b200_instance_desc;
 
 olb_b200_status olb_b200_ensemble_create(const olb_b200_ensemble_desc* desc, olb_b200_ensemble** out);
@@ -380,7 +386,8 @@ olb_b200_status olb_b200_ensemble_info(olb_b200_ensemble* ensemble, int64_t* poo
 /* Resident blocks per SM of the batched kernel (2, 3 or 4); the grid is that
  * many blocks per SM. */
 olb_b200_status olb_b200_ensemble_set_occupancy(olb_b200_ensemble* ensemble, int32_t blocks_per_sm);
-/* Pool bytes one instance of this extent occupies. */
+/* Pool bytes one instance of this extent occupies (a geometry instance adds
+ * its table: the cell count rounded up to 256 bytes). */
 uint64_t olb_b200_ensemble_bytes_per_instance(int32_t nx, int32_t ny, int32_t nz);
 
 /* Thread-local message of the last failed call on this thread ("" if none). */

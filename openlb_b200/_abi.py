@@ -52,7 +52,7 @@ EXPORTED = [
     "olb_b200_set_max_steps_in_flight", "olb_b200_set_force_field",
 ]
 
-ENSEMBLE_CAVITY, ENSEMBLE_CHANNEL = 1, 2
+ENSEMBLE_CAVITY, ENSEMBLE_CHANNEL, ENSEMBLE_GEOMETRY = 1, 2, 3
 
 
 class LibraryNotBuilt(RuntimeError):
@@ -115,7 +115,7 @@ class EnsembleDesc(ctypes.Structure):
 class InstanceDesc(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
                 ("nz", ctypes.c_int32), ("omega", ctypes.c_double), ("wall_u", ctypes.c_double * 3),
-                ("force", ctypes.c_double * 3)]
+                ("force", ctypes.c_double * 3), ("cells", ctypes.c_void_p)]
 
 
 _loaded: dict = {}

@@ -39,11 +39,15 @@ struct Geometry {
   // masked lattices: a box [lo, hi) whose cells all use the bulk entry, so the
   // step kernel skips their dynamics id (empty when lo == hi)
   int32_t bulk_lo[3], bulk_hi[3];
-  int32_t bulk_id;  // masked lattices: the table entry of the box cells
   // FORCE per cell for the Guo-forced dynamics (3 columns of `stride` values
   // of the compute type, natural cell order), or nullptr: the entries' forces
   const void* force;
 };
+
+// the entry index the masked kernels give a cell of the bulk box (the table
+// holds at most 256 entries): it collides with the bulk entry, the kernel
+// argument, and loads nothing from the table
+constexpr int kBoxCell = 256;
 
 OLB_HD bool in_bulk_box(const Geometry& g, int x, int y, int z)
 {
@@ -253,7 +257,7 @@ OLB_DEV void step_tile(S* __restrict__ pops, const Geometry& g, const DynDevice<
     if (go[k]) {
       n[k] = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
       if constexpr (MASKED) {
-        kind[k] = __ldg(&table[id[k]].kind);
+        if (id[k] != kBoxCell) kind[k] = __ldg(&table[id[k]].kind);
       }
       // full-way bounce-back is a no-op on the AA pattern (see file comment)
       go[k] = kind[k] != K_BOUNCE_BACK;
@@ -289,17 +293,28 @@ OLB_DEV void step_tile(S* __restrict__ pops, const Geometry& g, const DynDevice<
     bool counted = false;
     if (kind[k] == KIND) {
       if constexpr (MASKED) {
-        // the entry's collision constants
-        const DynDevice<R>* e = table + id[k];
+        // the entry's collision constants (the bulk entry's for box cells)
         DynDevice<R> q;
-        q.omega = __ldg(&e->omega);
-        q.omega_minus = __ldg(&e->omega_minus);
-        q.smago_pre = __ldg(&e->smago_pre);
-        q.tau_mol = __ldg(&e->tau_mol);
-        q.force[0] = __ldg(&e->force[0]);
-        q.force[1] = __ldg(&e->force[1]);
-        q.force[2] = __ldg(&e->force[2]);
-        q.force_relax = __ldg(&e->force_relax);
+        if (id[k] == kBoxCell) {
+          q.omega = bulk.omega;
+          q.omega_minus = bulk.omega_minus;
+          q.smago_pre = bulk.smago_pre;
+          q.tau_mol = bulk.tau_mol;
+          q.force[0] = bulk.force[0];
+          q.force[1] = bulk.force[1];
+          q.force[2] = bulk.force[2];
+          q.force_relax = bulk.force_relax;
+        } else {
+          const DynDevice<R>* e = table + id[k];
+          q.omega = __ldg(&e->omega);
+          q.omega_minus = __ldg(&e->omega_minus);
+          q.smago_pre = __ldg(&e->smago_pre);
+          q.tau_mol = __ldg(&e->tau_mol);
+          q.force[0] = __ldg(&e->force[0]);
+          q.force[1] = __ldg(&e->force[1]);
+          q.force[2] = __ldg(&e->force[2]);
+          q.force_relax = __ldg(&e->force_relax);
+        }
         if constexpr (kForced) {
           if (g.force) {
             q.force[0] = fc[k][0]; q.force[1] = fc[k][1]; q.force[2] = fc[k][2];
@@ -373,28 +388,44 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const DynDevice<R> bulk, 
 }
 
 // Tiles of the masked kernels: the blocks of step_grid() in launch order,
-// t = bx + tz * (by + ty * x); origin() gives a thread's first cell in tile t.
-struct TileGrid {
-  uint32_t tz, ty, tiles, rows;
-  OLB_DEV TileGrid(const Geometry& g, int cpt, int nx)
+// t = bx + tz * (by + ty * x).  A block starts at tile blockIdx.x and steps by
+// gridDim.x; the step is decomposed into tile coordinates once, so advancing
+// costs a few adds and two conditional carries instead of two divisions per
+// tile (a tile is one to two cells per thread).
+struct TileWalk {
+  uint32_t bx, by, x;     // current tile
+  uint32_t sbx, sby, sx;  // gridDim.x in tile coordinates (sbx < tz, sby < ty)
+  uint32_t tz, ty, rows;
+  OLB_DEV TileWalk(const Geometry& g, int cpt)
   {
     rows = blockDim.y * uint32_t(cpt);
     tz = (uint32_t(g.nz) + blockDim.x - 1) / blockDim.x;
     ty = (uint32_t(g.ny) + rows - 1) / rows;
-    tiles = tz * ty * uint32_t(nx);
+    uint32_t r = blockIdx.x / tz;
+    bx = blockIdx.x - r * tz;
+    x = r / ty;
+    by = r - x * ty;
+    r = gridDim.x / tz;
+    sbx = gridDim.x - r * tz;
+    sx = r / ty;
+    sby = r - sx * ty;
   }
-  OLB_DEV void origin(uint32_t t, int& x, int& y0, int& z) const
+  OLB_DEV void advance()
   {
-    const uint32_t r = t / tz;
-    const uint32_t xi = r / ty;
-    z = int((t - r * tz) * blockDim.x + threadIdx.x);
-    y0 = int((r - xi * ty) * rows + threadIdx.y);
-    x = int(xi);
+    bx += sbx;
+    const uint32_t cz = bx >= tz;
+    bx -= cz * tz;
+    by += sby + cz;
+    const uint32_t cy = by >= ty;
+    by -= cy * ty;
+    x += sx + cy;
   }
+  OLB_DEV int z() const { return int(bx * blockDim.x + threadIdx.x); }
+  OLB_DEV int y0() const { return int(by * rows + threadIdx.y); }
 };
 
-// table entries of a tile's cells: box cells use the bulk entry without a
-// load; cells outside the lattice get -1 (they are skipped)
+// table entries of a tile's cells: kBoxCell for cells of the bulk box (they
+// use the bulk entry, no load), -1 for cells outside the lattice (skipped)
 template <int CPT>
 OLB_DEV void load_tile_ids(int (&id)[CPT], const Geometry& g, const uint8_t* __restrict__ ids, int x, int y0,
                            int z, int dy)
@@ -404,7 +435,7 @@ OLB_DEV void load_tile_ids(int (&id)[CPT], const Geometry& g, const uint8_t* __r
     id[k] = -1;
     if (z < g.nz && y < g.ny) {
       id[k] = in_bulk_box(g, x, y, z)
-                ? g.bulk_id
+                ? kBoxCell
                 : int(ids[(uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z)]);
     }
   });
@@ -421,27 +452,18 @@ aa_step_masked_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __r
                       const DynDevice<R>* __restrict__ table, const DynDevice<R> bulk,
                       StatPartial* __restrict__ partials)
 {
-  const TileGrid tg(g, CPT, g.nx);
+  TileWalk w(g, CPT);
+  const uint32_t nx = uint32_t(g.nx);
   const int dy = int(blockDim.y);
   StatAcc acc;
   int next[CPT];
-  uint32_t t = blockIdx.x;
-  if (t < tg.tiles) {
-    int x, y0, z;
-    tg.origin(t, x, y0, z);
-    load_tile_ids(next, g, ids, x, y0, z, dy);
-  }
-  for (; t < tg.tiles; t += gridDim.x) {
+  if (w.x < nx) load_tile_ids(next, g, ids, int(w.x), w.y0(), w.z(), dy);
+  while (w.x < nx) {
     int cur[CPT];
     static_for<0, CPT>([&](auto k) { cur[k] = next[k]; });
-    const uint32_t tn = t + gridDim.x;
-    if (tn < tg.tiles) {
-      int xn, yn, zn;
-      tg.origin(tn, xn, yn, zn);
-      load_tile_ids(next, g, ids, xn, yn, zn, dy);
-    }
-    int x, y0, z;
-    tg.origin(t, x, y0, z);
+    const int x = int(w.x), y0 = w.y0(), z = w.z();
+    w.advance();
+    if (w.x < nx) load_tile_ids(next, g, ids, int(w.x), w.y0(), w.z(), dy);
     step_tile<Q, S, R, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, x, y0, z, dy, cur, acc);
   }
   if constexpr (STATS) {
@@ -601,8 +623,8 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
     if (go[k]) {
       e[k] = (uint32_t(xp) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
       if constexpr (MASKED) {
-        kind_lo[k] = __ldg(&table[id_lo[k]].kind);
-        kind_hi[k] = __ldg(&table[id_hi[k]].kind);
+        if (id_lo[k] != kBoxCell) kind_lo[k] = __ldg(&table[id_lo[k]].kind);
+        if (id_hi[k] != kBoxCell) kind_hi[k] = __ldg(&table[id_hi[k]].kind);
       }
       // two bounce-back cells: nothing to do (AA no-op)
       go[k] = !(kind_lo[k] == K_BOUNCE_BACK && kind_hi[k] == K_BOUNCE_BACK);
@@ -725,8 +747,10 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
       }
     };
     // the table entries (nullptr: the bulk entry, the kernel argument)
-    cell(std::integral_constant<bool, false>{}, kind_lo[k], MASKED ? table + id_lo[k] : nullptr);
-    cell(std::integral_constant<bool, true>{}, kind_hi[k], MASKED ? table + id_hi[k] : nullptr);
+    cell(std::integral_constant<bool, false>{}, kind_lo[k],
+         MASKED && id_lo[k] != kBoxCell ? table + id_lo[k] : nullptr);
+    cell(std::integral_constant<bool, true>{}, kind_hi[k],
+         MASKED && id_hi[k] != kBoxCell ? table + id_hi[k] : nullptr);
     // recomputed after the collision rather than kept live through it
     PairNeighbours nb(g, int(opaque(uint32_t(xp))), int(opaque(uint32_t(y))), int(opaque(uint32_t(z))));
     const uint32_t ps = opaque(pstride);
@@ -772,24 +796,22 @@ aa_step_masked_paired_kernel(S* __restrict__ pops, const Geometry g, const uint8
                              StatPartial* __restrict__ partials)
 {
   const int nxh = g.nx >> 1;
-  const TileGrid tg(g, CPT, nxh);
+  TileWalk w(g, CPT);
   const int dy = int(blockDim.y);
   StatAcc acc;
   int next_lo[CPT], next_hi[CPT];
-  auto fetch = [&](uint32_t t) {
-    int xp, y0, z;
-    tg.origin(t, xp, y0, z);
+  auto fetch = [&]() {
+    const int xp = int(w.x), y0 = w.y0(), z = w.z();
     load_tile_ids(next_lo, g, ids, xp, y0, z, dy);
     load_tile_ids(next_hi, g, ids, xp + nxh, y0, z, dy);
   };
-  uint32_t t = blockIdx.x;
-  if (t < tg.tiles) fetch(t);
-  for (; t < tg.tiles; t += gridDim.x) {
+  if (w.x < uint32_t(nxh)) fetch();
+  while (w.x < uint32_t(nxh)) {
     int lo[CPT], hi[CPT];
     static_for<0, CPT>([&](auto k) { lo[k] = next_lo[k]; hi[k] = next_hi[k]; });
-    if (t + gridDim.x < tg.tiles) fetch(t + gridDim.x);
-    int xp, y0, z;
-    tg.origin(t, xp, y0, z);
+    const int xp = int(w.x), y0 = w.y0(), z = w.z();
+    w.advance();
+    if (w.x < uint32_t(nxh)) fetch();
     paired_tile<Q, S, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, xp, y0, z, dy, lo, hi, acc);
   }
   if constexpr (STATS) {

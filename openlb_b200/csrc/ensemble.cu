@@ -10,9 +10,11 @@
 // flat index by multiply-shift division (Granlund & Montgomery, "Division by
 // invariant integers using multiplication", PLDI 1994) with per-instance
 // constants, so instances of any size share the launch without idle lanes.
-// Geometry is procedural: a lid-driven cavity (bounce-back box, moving lid on
-// the y = ny-1 face) or a channel (x periodic, bounce-back walls at the y and
-// z faces, Guo body force along x).  Per-instance relaxation, lid velocity and
+// An instance's geometry is its own table (one class byte per cell in its
+// pool region: fluid, bounce-back wall, moving wall; read with the cell's
+// populations) or procedural: a lid-driven cavity (bounce-back box, moving lid
+// on the y = ny-1 face) or a channel (x periodic, bounce-back walls at the y
+// and z faces, Guo body force along x).  Per-instance relaxation, lid velocity and
 // force come from the instance table.  A chunk can end with the
 // velocity-change residual of every instance (FP64 sums per tile, reduced per
 // instance in a fixed order, so results do not depend on the mix), in a pass
@@ -73,12 +75,14 @@ struct FastDiv {
 struct InstanceDevice {
   uint64_t pops;       // element offset of population column 0 in the pool
   uint64_t uprev;      // element offset of the stored velocity (3 columns)
+  uint64_t geom;       // element offset of the cell-class bytes (geometry instances), 0: procedural
   uint32_t stride;     // column length in elements
   uint32_t cells;
   int32_t nx, ny, nz;
   uint32_t nz_u, nynz;
   FastDiv div_nynz, div_nz;
-  int32_t kind;        // OLB_B200_ENSEMBLE_CAVITY / _CHANNEL
+  int32_t kind;        // OLB_B200_ENSEMBLE_CAVITY / _CHANNEL / _GEOMETRY
+  int32_t forced;      // fluid cells collide with Guo-forced BGK
   int32_t active;
   uint32_t steps_done; // steps completed before the current chunk
   float omega;
@@ -109,8 +113,12 @@ OLB_DEV uint32_t flat_offset(uint32_t nynz, uint32_t nz)
   return uint32_t(CX) * nynz + uint32_t(CY) * nz + uint32_t(CZ);
 }
 
-OLB_DEV int cell_kind(const InstanceDevice& I, int x, int y, int z)
+// the cell's class: the instance's geometry table, else its procedural geometry
+OLB_DEV int cell_kind(const float* __restrict__ pool, const InstanceDevice& I, uint32_t n, int x, int y, int z)
 {
+  if (I.geom) {
+    return int(__ldg(reinterpret_cast<const uint8_t*>(pool + I.geom) + n));
+  }
   if (I.kind == OLB_B200_ENSEMBLE_CAVITY) {
     if (x == 0 || x == I.nx - 1 || y == 0 || z == 0 || z == I.nz - 1) return CELL_WALL;
     return y == I.ny - 1 ? CELL_LID : CELL_FLUID;
@@ -145,7 +153,7 @@ ensemble_step_kernel(float* __restrict__ pool, const InstanceDevice* __restrict_
       const uint32_t r = n - x * I.nynz;
       const uint32_t y = I.div_nz.div(r);
       const uint32_t z = r - y * I.nz_u;
-      const int kind = cell_kind(I, int(x), int(y), int(z));
+      const int kind = cell_kind(pool, I, n, int(x), int(y), int(z));
       if (kind == CELL_WALL) continue;  // full-way bounce-back: AA no-op
       // Odd steps address neighbours.  A cell off every face of its box reaches
       // them without wrap-around: neighbour (x+cx, y+cy, z+cz) is the flat index
@@ -173,7 +181,7 @@ ensemble_step_kernel(float* __restrict__ pool, const InstanceDevice* __restrict_
       }
       if (kind == CELL_FLUID) {
         float rho, u[3];
-        if (I.kind == OLB_B200_ENSEMBLE_CHANNEL) {
+        if (I.forced) {
           const float gg[3] = {I.force[0], I.force[1], I.force[2]};
           float delta;
           compute_rho_delta_u_forced<L>(f, gg, rho, delta, u);
@@ -241,13 +249,13 @@ ensemble_check_kernel(float* __restrict__ pool, const InstanceDevice* __restrict
         const uint32_t r = n - x * I.nynz;
         const uint32_t y = I.div_nz.div(r);
         const uint32_t z = r - y * I.nz_u;
-        if (cell_kind(I, int(x), int(y), int(z)) != CELL_FLUID) continue;
+        if (cell_kind(pool, I, n, int(x), int(y), int(z)) != CELL_FLUID) continue;
         float f[kQ];
         static_for<0, kQ>([&](auto i) {
           f[i] = logical_pop<kQ, float, float, i.value>(pops, g, int(x), int(y), int(z), shifted);
         });
         float rho, u[3];
-        if (I.kind == OLB_B200_ENSEMBLE_CHANNEL) {
+        if (I.forced) {
           const float gg[3] = {I.force[0], I.force[1], I.force[2]};
           compute_rho_u_forced<L>(f, gg, rho, u);
         } else {
@@ -318,7 +326,7 @@ __global__ void ensemble_moments_kernel(const float* __restrict__ pool, Instance
   const uint32_t r = n - x * I.nynz;
   const uint32_t y = I.div_nz.div(r);
   const uint32_t z = r - y * I.nz_u;
-  const int kind = cell_kind(I, int(x), int(y), int(z));
+  const int kind = cell_kind(pool, I, n, int(x), int(y), int(z));
   float rho = 1.f, u[3] = {0.f, 0.f, 0.f};
   if (kind == CELL_LID) {
     u[0] = I.lid_u[0]; u[1] = I.lid_u[1]; u[2] = I.lid_u[2];
@@ -330,7 +338,7 @@ __global__ void ensemble_moments_kernel(const float* __restrict__ pool, Instance
     static_for<0, kQ>([&](auto i) {
       f[i] = logical_pop<kQ, float, float, i.value>(pops, g, int(x), int(y), int(z), shifted);
     });
-    if (I.kind == OLB_B200_ENSEMBLE_CHANNEL) {
+    if (I.forced) {
       const float gg[3] = {I.force[0], I.force[1], I.force[2]};
       compute_rho_u_forced<L>(f, gg, rho, u);
     } else {
@@ -622,11 +630,23 @@ olb_b200_status olb_b200_ensemble_add(olb_b200_ensemble* E, const olb_b200_insta
 {
   detail::set_last_error("");
   if (!E || !d || !slot_out) return efail(OLB_B200_ERR_ARG, "ensemble_add: null argument");
-  if (d->kind != OLB_B200_ENSEMBLE_CAVITY && d->kind != OLB_B200_ENSEMBLE_CHANNEL)
+  if (d->kind != OLB_B200_ENSEMBLE_CAVITY && d->kind != OLB_B200_ENSEMBLE_CHANNEL &&
+      d->kind != OLB_B200_ENSEMBLE_GEOMETRY)
     return efail(OLB_B200_ERR_ARG, "ensemble_add: unknown instance kind");
+  const bool table = d->kind == OLB_B200_ENSEMBLE_GEOMETRY;
+  if (table != (d->cells != nullptr))
+    return efail(OLB_B200_ERR_ARG, "ensemble_add: a geometry table is given exactly for geometry instances");
   if (d->nx < 3 || d->ny < 3 || d->nz < 3) return efail(OLB_B200_ERR_ARG, "ensemble_add: extent below 3");
   if (!(d->omega > 0.0 && d->omega < 2.0)) return efail(OLB_B200_ERR_ARG, "ensemble_add: omega outside (0,2)");
   const uint64_t cells = uint64_t(d->nx) * d->ny * d->nz;
+  if (table) {
+    for (uint64_t c = 0; c < cells; ++c) {
+      if (d->cells[c] > 2)
+        return efail(OLB_B200_ERR_ARG, "ensemble_add: cell " + std::to_string(c) + " has class " +
+                                         std::to_string(unsigned(d->cells[c])) +
+                                         " (0 fluid, 1 wall, 2 moving wall)");
+    }
+  }
   // the step kernel indexes an instance's populations with 32 bits
   if (instance_elems(cells) >= (uint64_t(1) << 32))
     return efail(OLB_B200_ERR_ARG, "ensemble_add: instance too large (q x cells must stay below 2^32)");
@@ -638,13 +658,21 @@ olb_b200_status olb_b200_ensemble_add(olb_b200_ensemble* E, const olb_b200_insta
     }
   }
   if (slot < 0) return efail(OLB_B200_ERR_OOM, "ensemble_add: no free instance slot");
-  const uint64_t need = instance_elems(cells);
+  // populations and stored velocity, then the geometry table (bytes, in
+  // whole 256-byte units)
+  const uint64_t table_elems = table ? round_up(cells, 256) / sizeof(float) : 0;
+  const uint64_t need = instance_elems(cells) + table_elems;
   uint64_t offset = 0;
   if (!pool_alloc(E, need, offset)) return efail(OLB_B200_ERR_OOM, "ensemble_add: HBM pool budget exhausted");
   OLB_ECUDA(cudaSetDevice(E->device));
   // rest state: shifted populations 0 = equilibrium at rho 1, u 0; stored velocity 0
   OLB_ECUDA(cudaMemsetAsync(E->pool + offset, 0, need * sizeof(float), E->stream));
   InstanceDevice I{};
+  if (table) {
+    I.geom = offset + instance_elems(cells);
+    OLB_ECUDA(cudaMemcpyAsync(E->pool + I.geom, d->cells, cells, cudaMemcpyHostToDevice, E->stream));
+    OLB_ECUDA(cudaStreamSynchronize(E->stream));  // the caller's table may go away after this call
+  }
   const uint32_t stride = uint32_t(round_up(cells, 64));
   I.pops = offset;
   I.uprev = offset + uint64_t(stride) * kQ;
@@ -658,6 +686,8 @@ olb_b200_status olb_b200_ensemble_add(olb_b200_ensemble* E, const olb_b200_insta
   I.div_nynz = FastDiv::make(I.nynz);
   I.div_nz = FastDiv::make(I.nz_u);
   I.kind = d->kind;
+  I.forced = d->kind == OLB_B200_ENSEMBLE_CHANNEL ||
+             (table && (d->force[0] != 0.0 || d->force[1] != 0.0 || d->force[2] != 0.0));
   I.active = 1;
   I.steps_done = 0;
   I.omega = float(d->omega);

@@ -304,8 +304,9 @@ OLB_DEV void relax_trt_reference(R (&f)[L::q], R rho, const R (&u)[3], R omega, 
 }
 
 // The equilibrium's momentum coefficient 3 w_i (with inv_cs2 = 3) applied to
-// x = rho (c_i . u) (times omega in the scaled form), with 3 w_i held as an
-// unevaluated sum hi + lo of two R values.  hi alone is biased: in FP32
+// x = rho (c_i . u), with 3 w_i held as an unevaluated sum hi + lo of two R
+// values (FP32 / FP64 storage; the 16-bit collisions keep one coefficient,
+// their storage rounding being far larger than its bias).  hi alone is biased: in FP32
 // fl(1/6) = fl(3/18) and fl(1/12) = fl(3/36) both exceed the exact value by
 // the same 3.0e-8 relative, so the equilibrium's momentum sum_i hi_i c_i c_i
 // rho u = (1 + 3.0e-8) rho u, and each relaxation adds omega times that bias
@@ -860,6 +861,7 @@ OLB_DEV void relax_bgk_scaled(float (&g)[L::q], float rho, float delta, const fl
   const float usqr = norm_sqr(u);
   const float e0 = -1.5f * usqr;
   const float keep = 1.f - omega;
+  const float omega_rho = omega * rho;
   {
     constexpr float T = storage_scale<L>(0) * weight<L, float>(0);
     const float wt = omega * T;
@@ -872,9 +874,11 @@ OLB_DEV void relax_bgk_scaled(float (&g)[L::q], float rho, float delta, const fl
     const float cu = c_dot<L, i.value>(u);
     const float ev = 4.5f * cu * cu + e0;
     const float a = wt * (delta + rho * ev);
-    // 3 s_i w_i omega (rho c.u): s_i is a power of two, so the scaled
-    // coefficient has the same hi + lo split as 3 w_i
-    const float b = storage_scale<L>(i) * momentum_term<L, float, i.value>(omega * (rho * cu));
+    // 3 s_i w_i omega rho c.u with one rounded coefficient: its relative
+    // bias (the hi + lo split of the FP32 path) is far below the 16-bit
+    // storage rounding, so the split would only cost instructions here
+    constexpr float K = 3.f * T;
+    const float b = K * (omega_rho * cu);
     g[i] = (keep * g[i] + a) + b;
     g[o] = (keep * g[o] + a) - b;
   });
@@ -896,7 +900,8 @@ OLB_DEV void relax_trt_scaled(float (&g)[L::q], float rho, float delta, const fl
     const float cu = c_dot<L, i.value>(u);
     const float ev = 4.5f * cu * cu + e0;
     const float a = T * (delta + rho * ev);
-    const float b = storage_scale<L>(i) * momentum_term<L, float, i.value>(rho * cu);
+    constexpr float K = 3.f * T;  // one rounded coefficient (see relax_bgk_scaled)
+    const float b = K * (rho * cu);
     const float dp = omega * (0.5f * (g[i] + g[o]) - a);
     const float dm = omega_minus * (0.5f * (g[i] - g[o]) - b);
     const float gi = g[i] - dp - dm;

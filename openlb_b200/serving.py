@@ -13,6 +13,10 @@ library's multi-step call.  All report solves/s and the p50/p99 latency
 (completion minus arrival).
 
     python -m openlb_b200.serving --requests 2000 --rate 50 --budget-gb 150 --plain
+
+Every instance carries its geometry as a table (one class byte per cell:
+fluid, bounce-back wall, moving wall) unless --procedural names the built-in
+cavity instead.
 """
 from __future__ import annotations
 
@@ -42,6 +46,7 @@ class Request:
     tol: float = 1e-7
     max_steps: int = 20000
     force: float = 0.0
+    geometry: np.ndarray | None = None  # kind ENSEMBLE_GEOMETRY: n^3 cell classes (0 fluid, 1 wall, 2 lid), z fastest
 
     @property
     def nu(self) -> float:
@@ -73,9 +78,12 @@ class Result:
 
 
 def make_requests(count: int, rate: float, seed: int = 0, n_range=(24, 96), re_range=(10.0, 400.0),
-                  lid_range=(0.05, 0.1), tol: float = 1e-7, max_steps: int = 20000) -> list:
+                  lid_range=(0.05, 0.1), tol: float = 1e-7, max_steps: int = 20000,
+                  tables: bool = False) -> list:
     """Cavity requests: side uniform in n_range, Re log-uniform, lid speed
-    uniform, Poisson arrivals at `rate` per second (0: all at t = 0)."""
+    uniform, Poisson arrivals at `rate` per second (0: all at t = 0).
+    tables: each request carries its geometry as a table (kind
+    ENSEMBLE_GEOMETRY) instead of naming the procedural cavity."""
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate, count) if rate > 0 else np.zeros(count)
     arrivals = np.cumsum(gaps) - (gaps[0] if count else 0.0)
@@ -84,7 +92,11 @@ def make_requests(count: int, rate: float, seed: int = 0, n_range=(24, 96), re_r
         n = int(rng.integers(n_range[0], n_range[1] + 1))
         re = float(math.exp(rng.uniform(math.log(re_range[0]), math.log(re_range[1]))))
         lid = float(rng.uniform(*lid_range))
-        out.append(Request(k, float(arrivals[k]), n, re, lid, tol=tol, max_steps=max_steps))
+        req = Request(k, float(arrivals[k]), n, re, lid, tol=tol, max_steps=max_steps)
+        if tables:
+            req.kind = _abi.ENSEMBLE_GEOMETRY
+            req.geometry = cavity((n, n, n))
+        out.append(req)
     return out
 
 
@@ -114,16 +126,25 @@ class Ensemble:
         except Exception:
             pass
 
-    def bytes_for(self, n: int) -> int:
-        return int(self._lib.olb_b200_ensemble_bytes_per_instance(n, n, n))
+    def bytes_for(self, n: int, table: bool = False) -> int:
+        """Pool bytes of an instance of side n (with a geometry table: + n^3
+        rounded up to 256)."""
+        extra = -(-n ** 3 // 256) * 256 if table else 0
+        return int(self._lib.olb_b200_ensemble_bytes_per_instance(n, n, n)) + extra
 
     def add(self, req: Request) -> int | None:
         """Admit a request; None when no slot or pool memory is free."""
         d = _abi.InstanceDesc()
         d.kind, d.nx, d.ny, d.nz = req.kind, req.n, req.n, req.n
         d.omega = req.omega
-        d.wall_u[0] = req.lid if req.kind == _abi.ENSEMBLE_CAVITY else 0.0
+        d.wall_u[0] = req.lid if req.kind in (_abi.ENSEMBLE_CAVITY, _abi.ENSEMBLE_GEOMETRY) else 0.0
         d.force[0] = req.force
+        cells = None
+        if req.kind == _abi.ENSEMBLE_GEOMETRY:
+            cells = np.ascontiguousarray(req.geometry, dtype=np.uint8).reshape(-1)
+            if cells.size != req.cells:
+                raise ValueError(f"geometry table has {cells.size} cells, the instance {req.cells}")
+            d.cells = cells.ctypes.data
         slot = ctypes.c_int32()
         st = self._lib.olb_b200_ensemble_add(self._h, ctypes.byref(d), ctypes.byref(slot))
         if st == _abi.ERR_OOM:
@@ -207,9 +228,18 @@ def serve_batched(requests: list, pool_bytes: int, max_instances: int = 1024, ch
 
 def cavity_lattice(req: Request, device: int = 0) -> Lattice:
     """The request's lattice on the single-lattice API (same geometry and
-    dynamics as the ensemble's procedural instance)."""
+    dynamics as the ensemble's instance)."""
     n = req.n
-    if req.kind == _abi.ENSEMBLE_CAVITY:
+    if req.kind == _abi.ENSEMBLE_GEOMETRY:
+        ids = np.ascontiguousarray(req.geometry, dtype=np.uint8).reshape(n, n, n)
+        # an axis is periodic where fluid reaches its faces (the instance wraps every axis)
+        periodic = tuple(bool(np.any(np.take(ids, 0, axis=a) == 0) or np.any(np.take(ids, -1, axis=a) == 0))
+                         for a in range(3))
+        fluid = (ForcedBGKdynamics(omega=req.omega, force=(req.force, 0.0, 0.0)) if req.force != 0.0
+                 else BGKdynamics(omega=req.omega))
+        lat = Lattice(19, (n, n, n), periodic, storage="f32", device=device)
+        lat.set_dynamics([fluid, BounceBack(), BounceBackVelocity((req.lid, 0.0, 0.0))], ids.reshape(-1))
+    elif req.kind == _abi.ENSEMBLE_CAVITY:
         lat = Lattice(19, (n, n, n), (False, False, False), storage="f32", device=device)
         lat.set_dynamics([BGKdynamics(omega=req.omega), BounceBack(), BounceBackVelocity((req.lid, 0.0, 0.0))],
                          cavity((n, n, n)))
@@ -295,9 +325,11 @@ def main(argv=None):
     ap.add_argument("--max-instances", type=int, default=4096)
     ap.add_argument("--occupancy", type=int, default=4)
     ap.add_argument("--plain", action="store_true", help="also run the plain one-at-a-time loops")
+    ap.add_argument("--procedural", action="store_true",
+                    help="instances name the built-in cavity instead of carrying geometry tables")
     args = ap.parse_args(argv)
     reqs = make_requests(args.requests, args.rate, args.seed, (args.nmin, args.nmax), tol=args.tol,
-                         max_steps=args.max_steps)
+                         max_steps=args.max_steps, tables=not args.procedural)
     out = {"config": vars(args), "cell_steps_total": None}
     b = serve_batched(reqs, int(args.budget_gb * 2 ** 30), args.max_instances, args.check,
                       occupancy=args.occupancy)

@@ -61,3 +61,14 @@ def test_pool_bytes_per_instance():
         assert lib.olb_b200_ensemble_bytes_per_instance(n, n, n) == stride * (19 + 3) * 4
     # the 150 GB budget holds 1900+ cavities of the largest size at once
     assert 150 * 2 ** 30 // lib.olb_b200_ensemble_bytes_per_instance(96, 96, 96) > 1900
+
+
+def test_table_requests_carry_the_cavity_geometry():
+    from openlb_b200.workloads import cavity
+    reqs = serving.make_requests(5, rate=10.0, seed=3, n_range=(12, 20), tables=True)
+    for r in reqs:
+        assert r.kind == _abi.ENSEMBLE_GEOMETRY
+        assert np.array_equal(r.geometry, cavity((r.n, r.n, r.n)))
+    plain = serving.make_requests(5, rate=10.0, seed=3, n_range=(12, 20))
+    assert [(r.n, r.re, r.lid, r.arrival) for r in plain] == [(r.n, r.re, r.lid, r.arrival) for r in reqs]
+    assert all(r.kind == _abi.ENSEMBLE_CAVITY and r.geometry is None for r in plain)
