@@ -194,6 +194,8 @@ def ncu_traffic(kernel_tag: str):
     """dram bytes per launch from a committed ncu summary, or None."""
     p = ROOT / "profiles" / f"{kernel_tag}.txt"
     if not p.exists():
+        p = p.with_suffix(".md")
+    if not p.exists():
         return None
     for line in p.read_text().splitlines():
         if line.startswith("dram_bytes_per_launch:"):
@@ -261,7 +263,9 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = measured_hbm_peak()
     bpc = 2 * q * BYTES_PER_CELL[storage]
     achieved = cells * bpc / (sec / args.steps) / 1e9
-    tag = f"aa_step_kernel_{WORKLOAD['name']}" if (n, q, storage) == (256, 19, "f32") else None
+    # the committed ncu summaries of the kernels the two bench arms time
+    tag = {(256, 19, "f32"): f"aa_step_kernel_{WORKLOAD['name']}",
+           (256, 19, "f16"): "aa_step_paired_kernel_f16_256"}.get((n, q, storage))
     traffic = ncu_traffic(tag) if tag else None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,

@@ -247,8 +247,10 @@ OLB_DEV void step_tile(S* __restrict__ pops, const Geometry& g, const DynDevice<
   bool go[CPT];
   uint32_t n[CPT];
 
-  // phase 1: classify the cells and issue all their loads (full-way
-  // bounce-back moves no bytes)
+  // phase 1: issue all loads.  Masked lattices load every cell's populations
+  // before its dynamics id has arrived (the id and the populations travel
+  // together instead of one after the other); a full-way bounce-back cell
+  // then stores nothing, its AA update being a no-op (see file comment).
   static_for<0, CPT>([&](auto k) {
     const int y = y0 + k.value * dy;
     go[k] = z < g.nz && y < g.ny;
@@ -256,13 +258,6 @@ OLB_DEV void step_tile(S* __restrict__ pops, const Geometry& g, const DynDevice<
     n[k] = 0;
     if (go[k]) {
       n[k] = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
-      if constexpr (MASKED) {
-        if (id[k] != kBoxCell) kind[k] = __ldg(&table[id[k]].kind);
-      }
-      // full-way bounce-back is a no-op on the AA pattern (see file comment)
-      go[k] = kind[k] != K_BOUNCE_BACK;
-    }
-    if (go[k]) {
       Neighbours nb(g, x, y, z);
       static_for<0, Q>([&](auto i) {
         if constexpr (!ODD) {
@@ -284,6 +279,12 @@ OLB_DEV void step_tile(S* __restrict__ pops, const Geometry& g, const DynDevice<
       }
     }
   });
+  if constexpr (MASKED) {
+    static_for<0, CPT>([&](auto k) {
+      if (go[k] && id[k] != kBoxCell) kind[k] = __ldg(&table[id[k]].kind);
+      go[k] = go[k] && kind[k] != K_BOUNCE_BACK;
+    });
+  }
 
   // phase 2: collide and store
   static_for<0, CPT>([&](auto k) {
@@ -387,43 +388,6 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const DynDevice<R> bulk, 
   }
 }
 
-// Tiles of the masked kernels: the blocks of step_grid() in launch order,
-// t = bx + tz * (by + ty * x).  A block starts at tile blockIdx.x and steps by
-// gridDim.x; the step is decomposed into tile coordinates once, so advancing
-// costs a few adds and two conditional carries instead of two divisions per
-// tile (a tile is one to two cells per thread).
-struct TileWalk {
-  uint32_t bx, by, x;     // current tile
-  uint32_t sbx, sby, sx;  // gridDim.x in tile coordinates (sbx < tz, sby < ty)
-  uint32_t tz, ty, rows;
-  OLB_DEV TileWalk(const Geometry& g, int cpt)
-  {
-    rows = blockDim.y * uint32_t(cpt);
-    tz = (uint32_t(g.nz) + blockDim.x - 1) / blockDim.x;
-    ty = (uint32_t(g.ny) + rows - 1) / rows;
-    uint32_t r = blockIdx.x / tz;
-    bx = blockIdx.x - r * tz;
-    x = r / ty;
-    by = r - x * ty;
-    r = gridDim.x / tz;
-    sbx = gridDim.x - r * tz;
-    sx = r / ty;
-    sby = r - sx * ty;
-  }
-  OLB_DEV void advance()
-  {
-    bx += sbx;
-    const uint32_t cz = bx >= tz;
-    bx -= cz * tz;
-    by += sby + cz;
-    const uint32_t cy = by >= ty;
-    by -= cy * ty;
-    x += sx + cy;
-  }
-  OLB_DEV int z() const { return int(bx * blockDim.x + threadIdx.x); }
-  OLB_DEV int y0() const { return int(by * rows + threadIdx.y); }
-};
-
 // table entries of a tile's cells: kBoxCell for cells of the bulk box (they
 // use the bulk entry, no load), -1 for cells outside the lattice (skipped)
 template <int CPT>
@@ -441,31 +405,23 @@ OLB_DEV void load_tile_ids(int (&id)[CPT], const Geometry& g, const uint8_t* __r
   });
 }
 
-// Masked lattices: a persistent grid of masked_grid() blocks walks the tiles
-// with a stride of gridDim.x.  A cell's dynamics id must be read before its
-// populations can be (bounce-back cells load none), so each block issues the
-// ids of its next tile before the populations of the current one: the id
-// latency overlaps a tile of work instead of preceding every population load.
+// Masked lattices: one tile per block, grid step_grid().  The ids of the
+// thread's cells are loaded first (none for cells of the bulk box); the
+// populations follow without waiting for them (step_tile).
 template <int Q, class S, class R, int KIND, bool ODD, bool STATS, int CPT, int MINB>
 __global__ void __launch_bounds__(kStepThreads, MINB)
 aa_step_masked_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict__ ids,
                       const DynDevice<R>* __restrict__ table, const DynDevice<R> bulk,
                       StatPartial* __restrict__ partials)
 {
-  TileWalk w(g, CPT);
-  const uint32_t nx = uint32_t(g.nx);
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
+  const int x = blockIdx.z;
   const int dy = int(blockDim.y);
+  int id[CPT];
+  load_tile_ids(id, g, ids, x, y0, z, dy);
   StatAcc acc;
-  int next[CPT];
-  if (w.x < nx) load_tile_ids(next, g, ids, int(w.x), w.y0(), w.z(), dy);
-  while (w.x < nx) {
-    int cur[CPT];
-    static_for<0, CPT>([&](auto k) { cur[k] = next[k]; });
-    const int x = int(w.x), y0 = w.y0(), z = w.z();
-    w.advance();
-    if (w.x < nx) load_tile_ids(next, g, ids, int(w.x), w.y0(), w.z(), dy);
-    step_tile<Q, S, R, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, x, y0, z, dy, cur, acc);
-  }
+  step_tile<Q, S, R, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, x, y0, z, dy, id, acc);
   if constexpr (STATS) {
     block_stats(acc.rho, acc.usqr, acc.max, acc.n, acc.nf, partials);
   }
@@ -621,15 +577,9 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
     kind_lo[k] = kind_hi[k] = KIND;
     e[k] = 0;
     if (go[k]) {
+      // the pair's populations are loaded before its ids have arrived (as in
+      // step_tile); a pair of two bounce-back cells then stores nothing
       e[k] = (uint32_t(xp) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
-      if constexpr (MASKED) {
-        if (id_lo[k] != kBoxCell) kind_lo[k] = __ldg(&table[id_lo[k]].kind);
-        if (id_hi[k] != kBoxCell) kind_hi[k] = __ldg(&table[id_hi[k]].kind);
-      }
-      // two bounce-back cells: nothing to do (AA no-op)
-      go[k] = !(kind_lo[k] == K_BOUNCE_BACK && kind_hi[k] == K_BOUNCE_BACK);
-    }
-    if (go[k]) {
       PairNeighbours nb(g, xp, y, z);
       static_for<0, Q>([&](auto i) {
         // 32-bit element indices: the paired layout is only used while
@@ -649,6 +599,15 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
       });
     }
   });
+  if constexpr (MASKED) {
+    static_for<0, CPT>([&](auto k) {
+      if (go[k]) {
+        if (id_lo[k] != kBoxCell) kind_lo[k] = __ldg(&table[id_lo[k]].kind);
+        if (id_hi[k] != kBoxCell) kind_hi[k] = __ldg(&table[id_hi[k]].kind);
+        go[k] = !(kind_lo[k] == K_BOUNCE_BACK && kind_hi[k] == K_BOUNCE_BACK);
+      }
+    });
+  }
 
   static_for<0, CPT>([&](auto k) {
     if (!go[k]) return;
@@ -788,32 +747,22 @@ aa_step_paired_kernel(S* __restrict__ pops, const Geometry g, const DynDevice<fl
   }
 }
 
-// the masked paired kernel: persistent, ids one tile ahead (aa_step_masked_kernel)
+// the masked paired kernel: one tile per block (aa_step_masked_kernel)
 template <int Q, class S, int KIND, bool ODD, bool STATS, int CPT, int MINB>
 __global__ void __launch_bounds__(kStepThreads, MINB)
 aa_step_masked_paired_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict__ ids,
                              const DynDevice<float>* __restrict__ table, const DynDevice<float> bulk,
                              StatPartial* __restrict__ partials)
 {
-  const int nxh = g.nx >> 1;
-  TileWalk w(g, CPT);
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
+  const int xp = blockIdx.z;
   const int dy = int(blockDim.y);
+  int lo[CPT], hi[CPT];
+  load_tile_ids(lo, g, ids, xp, y0, z, dy);
+  load_tile_ids(hi, g, ids, xp + (g.nx >> 1), y0, z, dy);
   StatAcc acc;
-  int next_lo[CPT], next_hi[CPT];
-  auto fetch = [&]() {
-    const int xp = int(w.x), y0 = w.y0(), z = w.z();
-    load_tile_ids(next_lo, g, ids, xp, y0, z, dy);
-    load_tile_ids(next_hi, g, ids, xp + nxh, y0, z, dy);
-  };
-  if (w.x < uint32_t(nxh)) fetch();
-  while (w.x < uint32_t(nxh)) {
-    int lo[CPT], hi[CPT];
-    static_for<0, CPT>([&](auto k) { lo[k] = next_lo[k]; hi[k] = next_hi[k]; });
-    const int xp = int(w.x), y0 = w.y0(), z = w.z();
-    w.advance();
-    if (w.x < uint32_t(nxh)) fetch();
-    paired_tile<Q, S, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, xp, y0, z, dy, lo, hi, acc);
-  }
+  paired_tile<Q, S, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, xp, y0, z, dy, lo, hi, acc);
   if constexpr (STATS) {
     block_stats(acc.rho, acc.usqr, acc.max, acc.n, acc.nf, partials);
   }
@@ -1302,7 +1251,6 @@ struct StepLaunch {
   StatPartial* partials;   // device, gridDim product entries
   int block_z, block_y;
   int variant;             // index into kStepVariants
-  int sm_count;            // multiprocessors of the device (masked_grid)
   cudaStream_t stream;
 };
 
@@ -1340,17 +1288,6 @@ inline dim3 step_grid(const Geometry& g, int bz, int by, int cells_per_thread)
 {
   const int rows = by * cells_per_thread;
   return dim3((g.nz + bz - 1) / bz, (g.ny + rows - 1) / rows, g.paired ? g.nx / 2 : g.nx);
-}
-
-// Grid of the persistent masked kernels: as many blocks as are resident at
-// once — min_blocks per multiprocessor, which __launch_bounds__ guarantees —
-// and no more than there are tiles.
-inline unsigned masked_grid(const Geometry& g, int bz, int by, int cells_per_thread, int min_blocks, int sm_count)
-{
-  const dim3 grid = step_grid(g, bz, by, cells_per_thread);
-  const size_t tiles = size_t(grid.x) * grid.y * grid.z;
-  const size_t resident = size_t(sm_count > 0 ? sm_count : 1) * size_t(min_blocks);
-  return unsigned(tiles < resident ? tiles : resident);
 }
 
 // grid of the gather / moments kernels (one cell per thread)

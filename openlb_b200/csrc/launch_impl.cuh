@@ -14,12 +14,12 @@ template <int Q, class S, class R, int KIND, int CPT, int MINB>
 static cudaError_t launch_step_variant(const StepLaunch& a, bool odd, bool masked, bool stats)
 {
   const dim3 block(a.block_z, a.block_y);
+  const dim3 grid = step_grid(a.g, a.block_z, a.block_y, CPT);
   S* pops = static_cast<S*>(a.pops);
   const DynDevice<R>* table = static_cast<const DynDevice<R>*>(a.table);
   const DynDevice<R>& bulk = *static_cast<const DynDevice<R>*>(a.bulk);
   constexpr bool kHalf = std::is_same_v<S, __half> || std::is_same_v<S, __nv_bfloat16>;
   if (masked) {
-    const dim3 grid(masked_grid(a.g, a.block_z, a.block_y, CPT, MINB, a.sm_count));
 #define OLB_LAUNCH(O, ST)                                                                          \
   do {                                                                                             \
     if constexpr (kHalf) {                                                                         \
@@ -39,7 +39,6 @@ static cudaError_t launch_step_variant(const StepLaunch& a, bool odd, bool maske
     }
 #undef OLB_LAUNCH
   } else {
-    const dim3 grid = step_grid(a.g, a.block_z, a.block_y, CPT);
 #define OLB_LAUNCH(O, ST)                                                                          \
   do {                                                                                             \
     if constexpr (kHalf) {                                                                         \

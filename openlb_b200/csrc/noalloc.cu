@@ -173,7 +173,6 @@ extern "C" olb_b200_status olb_b200_collide_and_stream_noalloc(
     a.block_z = bz;
     a.block_y = by;
     a.variant = variant;
-    a.sm_count = 0;  // unmasked lattices only: the masked grid is not used
     a.stream = s;
     const bool odd = ((steps_done + k) & 1) != 0;
     switch (desc->storage) {

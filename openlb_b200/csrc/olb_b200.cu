@@ -264,7 +264,6 @@ struct olb_b200_lattice {
   StatPartial* stat_host = nullptr;  // pinned
   int block_z = 0, block_y = 0;
   int variant = 0;          // index into kStepVariants
-  int sm_count = 0;         // multiprocessors of the device (grid of the masked kernels)
   void* force = nullptr;    // FORCE per cell, 3 columns of `stride` R (olb_b200_set_force_field)
   bool tuned = false;       // variant and shape chosen by olb_b200_autotune
   float tuned_ms = 0.f;
@@ -356,10 +355,6 @@ size_t boundary_blocks(const olb_b200_lattice* L)
 
 size_t step_blocks(const olb_b200_lattice* L)
 {
-  if (L->masked) {
-    return masked_grid(L->g, L->block_z, L->block_y, cells_per_thread(L), kStepVariants[L->variant].min_blocks,
-                       L->sm_count);
-  }
   const dim3 grid = step_grid(L->g, L->block_z, L->block_y, cells_per_thread(L));
   return size_t(grid.x) * grid.y * grid.z;
 }
@@ -471,7 +466,6 @@ olb_b200_status enqueue_steps(olb_b200_lattice* L, int steps, bool stats_last)
     a.block_z = L->block_z;
     a.block_y = L->block_y;
     a.variant = L->variant;
-    a.sm_count = L->sm_count;
     a.stream = L->stream;
     const bool odd = L->parity == 1;
     cudaError_t e = cudaSuccess;
@@ -704,7 +698,6 @@ olb_b200_status olb_b200_create(const olb_b200_desc* desc, olb_b200_lattice** ou
     cudaError_t e_ = (call);                                                                       \
     if (e_ != cudaSuccess) return cleanup(cuda_fail(e_, #call));                                   \
   } while (0)
-  OLB_CUDA_C(cudaDeviceGetAttribute(&L->sm_count, cudaDevAttrMultiProcessorCount, L->device));
   OLB_CUDA_C(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
   OLB_CUDA_C(cudaEventCreate(&L->ev0));
   OLB_CUDA_C(cudaEventCreate(&L->ev1));

@@ -172,7 +172,8 @@ def obstacle_geometry(n, seed, channel=False):
 
 def table_request(rid, n, seed, channel=False, **kw):
     kw.setdefault("re", 60.0)
-    kw.setdefault("lid", 0.0 if channel else 0.08)
+    # the channel has no moving wall; its lid speed only sets the viscosity (nu = lid n / Re)
+    kw.setdefault("lid", 0.05 if channel else 0.08)
     req = serving.Request(rid, 0.0, n=n, kind=_abi.ENSEMBLE_GEOMETRY, **kw)
     req.geometry = obstacle_geometry(n, seed, channel)
     return req
