@@ -201,6 +201,15 @@ olb_b200_status olb_b200_set_boundary_noise(olb_b200_lattice* lattice, double am
  * calls do nothing.  Synchronous. */
 olb_b200_status olb_b200_initialize(olb_b200_lattice* lattice);
 
+/* Every cell's populations set to the second-order equilibrium of its density
+ * and velocity — replaces SuperLattice::iniEquilibrium over the whole lattice
+ * (src/core/superLattice.hh:542-577; Cell::iniEquilibrium with
+ * equilibrium::secondOrder, src/dynamics/lbm.h:50-64), with the expansion done
+ * on the device: 4 values per cell cross PCIe instead of q.  rho holds one
+ * value per cell, u three columns (x of every cell, then y, then z), both of
+ * the ABI element type, cells in the populations' order.  Synchronous. */
+olb_b200_status olb_b200_ini_equilibrium(olb_b200_lattice* lattice, const void* rho, const void* u);
+
 /* Full population state, host <-> device — replaces
  * setProcessingContext(Simulation/Evaluation) for POPULATION
  * (src/core/platform/gpu/cuda/column.hh:157-187,285-296).  Logical layout. */

@@ -49,7 +49,7 @@ EXPORTED = [
     "olb_b200_ensemble_remove", "olb_b200_ensemble_run", "olb_b200_ensemble_get_moments",
     "olb_b200_ensemble_info", "olb_b200_ensemble_set_occupancy", "olb_b200_ensemble_bytes_per_instance",
     "olb_b200_set_boundary_values", "olb_b200_initialize", "olb_b200_set_boundary_noise",
-    "olb_b200_set_max_steps_in_flight", "olb_b200_set_force_field",
+    "olb_b200_set_max_steps_in_flight", "olb_b200_set_force_field", "olb_b200_ini_equilibrium",
 ]
 
 ENSEMBLE_CAVITY, ENSEMBLE_CHANNEL, ENSEMBLE_GEOMETRY = 1, 2, 3
@@ -150,6 +150,8 @@ def load(variant: str = "fast") -> ctypes.CDLL:
     lib.olb_b200_set_dynamics.restype = st
     lib.olb_b200_set_populations.argtypes = [P, P]
     lib.olb_b200_set_populations.restype = st
+    lib.olb_b200_ini_equilibrium.argtypes = [P, P, P]
+    lib.olb_b200_ini_equilibrium.restype = st
     lib.olb_b200_get_populations.argtypes = [P, P]
     lib.olb_b200_get_populations.restype = st
     lib.olb_b200_collide_and_stream.argtypes = [P, ctypes.c_int32, ctypes.POINTER(Stats)]

@@ -828,6 +828,30 @@ __global__ void scatter_natural_kernel(S* __restrict__ pops, const Geometry g,
   });
 }
 
+// Cell::iniEquilibrium on every cell: the second-order equilibrium of the
+// cell's density and velocity (equilibrium::secondOrder, src/dynamics/lbm.h:50-64,
+// as the shifted value f_eq - w), written in the natural layout; rho_u holds
+// rho of every cell, then u_x, u_y, u_z.
+template <int Q, class S, class R>
+__global__ void equilibrium_kernel(S* __restrict__ pops, const Geometry g, const R* __restrict__ rho_u)
+{
+  using L = Lattice<Q>;
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int x = blockIdx.z;
+  if (z >= g.nz || y >= g.ny) return;
+  const uint32_t n = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
+  const size_t cells = size_t(g.nx) * g.ny * g.nz;
+  const uint32_t slot = cell_slot(g, x, y, z);
+  const R rho = rho_u[n];
+  const R u[3] = {rho_u[cells + n], rho_u[2 * cells + n], rho_u[3 * cells + n]};
+  const R usqr = norm_sqr(u);
+  static_for<0, Q>([&](auto i) {
+    Store<S, R>::template store<L, i.value>(pops + size_t(i.value) * g.stride + slot,
+                                            feq2<L, i.value>(rho, u, usqr));
+  });
+}
+
 // FORCE of cell n of a Guo-forced dynamics: the lattice's force field when it
 // has one, else the entry's constant
 template <class R>
@@ -1264,6 +1288,10 @@ cudaError_t launch_gather(const void* pops, const Geometry& g, bool shifted, voi
 template <int Q, class S, class R>
 cudaError_t launch_scatter(void* pops, const Geometry& g, const void* in, int i_begin, int i_end,
                            cudaStream_t stream);
+
+// every cell's populations from its density and velocity (rho_u: 4 columns of R)
+template <int Q, class S, class R>
+cudaError_t launch_equilibrium(void* pops, const Geometry& g, const void* rho_u, cudaStream_t stream);
 
 template <int Q, class S, class R>
 cudaError_t launch_moments(const void* pops, const Geometry& g, bool shifted, const uint8_t* ids,

@@ -112,6 +112,15 @@ cudaError_t launch_scatter(void* pops, const Geometry& g, const void* in, int i_
 }
 
 template <int Q, class S, class R>
+cudaError_t launch_equilibrium(void* pops, const Geometry& g, const void* rho_u, cudaStream_t stream)
+{
+  const dim3 block(32, 8);
+  const dim3 grid = cell_grid(g, 32, 8);
+  equilibrium_kernel<Q, S, R><<<grid, block, 0, stream>>>(static_cast<S*>(pops), g, static_cast<const R*>(rho_u));
+  return cudaGetLastError();
+}
+
+template <int Q, class S, class R>
 cudaError_t launch_moments(const void* pops, const Geometry& g, bool shifted, const uint8_t* ids,
                            const void* table, void* rho, void* u, cudaStream_t stream)
 {
@@ -194,6 +203,7 @@ cudaError_t launch_boundary(void* pops, const Geometry& g, bool shifted, const u
                                               cudaStream_t);                                       \
   template cudaError_t launch_scatter<Q, S, R>(void*, const Geometry&, const void*, int, int,      \
                                                cudaStream_t);                                      \
+  template cudaError_t launch_equilibrium<Q, S, R>(void*, const Geometry&, const void*, cudaStream_t); \
   template cudaError_t launch_moments<Q, S, R>(const void*, const Geometry&, bool, const uint8_t*, \
                                                const void*, void*, void*, cudaStream_t);           \
   template cudaError_t launch_boundary_collide<Q, S, R>(void*, const Geometry&, bool, const uint8_t*, \

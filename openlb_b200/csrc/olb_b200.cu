@@ -27,6 +27,8 @@ namespace olb_b200 {
                                                      int, int, cudaStream_t);                      \
   extern template cudaError_t launch_scatter<Q, S, R>(void*, const Geometry&, const void*, int,    \
                                                       int, cudaStream_t);                          \
+  extern template cudaError_t launch_equilibrium<Q, S, R>(void*, const Geometry&, const void*,    \
+                                                          cudaStream_t);                           \
   extern template cudaError_t launch_moments<Q, S, R>(const void*, const Geometry&, bool,          \
                                                       const uint8_t*, const void*, void*, void*,   \
                                                       cudaStream_t);                               \
@@ -897,6 +899,27 @@ olb_b200_status olb_b200_set_populations(olb_b200_lattice* L, const void* host_p
       if (e != cudaSuccess) return cuda_fail(e, "scatter kernel");
     }
   }
+  OLB_CUDA(cudaStreamSynchronize(L->stream));
+  L->parity = 0;
+  return OLB_B200_OK;
+}
+
+olb_b200_status olb_b200_ini_equilibrium(olb_b200_lattice* L, const void* rho, const void* u)
+{
+  g_last_error.clear();
+  if (!L || !rho || !u) return fail(OLB_B200_ERR_ARG, "ini_equilibrium: null argument");
+  olb_b200_status st = select_device(L);
+  if (st != OLB_B200_OK) return st;
+  // rho and u staged in the scratch buffer (4 columns of R), expanded on the device
+  const size_t col = L->cells * L->real;
+  char* stage = static_cast<char*>(L->scratch);
+  OLB_CUDA(cudaMemcpyAsync(stage, rho, col, cudaMemcpyHostToDevice, L->stream));
+  OLB_CUDA(cudaMemcpyAsync(stage + col, u, 3 * col, cudaMemcpyHostToDevice, L->stream));
+  cudaError_t e = dispatch(L, [&](auto qc, auto s_, auto r_) {
+    return launch_equilibrium<decltype(qc)::value, decltype(s_), decltype(r_)>(L->pops, L->g, L->scratch,
+                                                                              L->stream);
+  });
+  if (e != cudaSuccess) return cuda_fail(e, "equilibrium kernel");
   OLB_CUDA(cudaStreamSynchronize(L->stream));
   L->parity = 0;
   return OLB_B200_OK;

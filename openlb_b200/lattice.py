@@ -279,6 +279,16 @@ class Lattice:
             raise ValueError(f"populations need {self.q * self.n} values, got {pops.size}")
         self._check(self._lib.olb_b200_set_populations(self._h, pops.ctypes.data))
 
+    def ini_equilibrium(self, rho: np.ndarray, u: np.ndarray) -> None:
+        """Every cell's populations from its density (cells) and velocity
+        (3, cells): the second-order equilibrium, computed on the device
+        (olb_b200_ini_equilibrium)."""
+        rho = np.ascontiguousarray(rho, dtype=self.dtype).reshape(-1)
+        u = np.ascontiguousarray(u, dtype=self.dtype).reshape(-1)
+        if rho.size != self.n or u.size != 3 * self.n:
+            raise ValueError(f"need {self.n} densities and {3 * self.n} velocity values")
+        self._check(self._lib.olb_b200_ini_equilibrium(self._h, rho.ctypes.data, u.ctypes.data))
+
     def _out(self, arr, count):
         if arr is None:
             return np.empty(count, self.dtype)
