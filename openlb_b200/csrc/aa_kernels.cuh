@@ -39,6 +39,7 @@ struct Geometry {
   // masked lattices: a box [lo, hi) whose cells all use the bulk entry, so the
   // step kernel skips their dynamics id (empty when lo == hi)
   int32_t bulk_lo[3], bulk_hi[3];
+  int32_t bulk_id;  // masked lattices: the table index of the bulk entry (-1: none)
   // FORCE per cell for the Guo-forced dynamics (3 columns of `stride` values
   // of the compute type, natural cell order), or nullptr: the entries' forces
   const void* force;
@@ -388,8 +389,9 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const DynDevice<R> bulk, 
   }
 }
 
-// table entries of a tile's cells: kBoxCell for cells of the bulk box (they
-// use the bulk entry, no load), -1 for cells outside the lattice (skipped)
+// table entries of a tile's cells: kBoxCell for cells of the bulk box and
+// cells of the bulk entry (they use the kernel argument, no table load), -1 for
+// cells outside the lattice (skipped)
 template <int CPT>
 OLB_DEV void load_tile_ids(int (&id)[CPT], const Geometry& g, const uint8_t* __restrict__ ids, int x, int y0,
                            int z, int dy)
@@ -398,9 +400,12 @@ OLB_DEV void load_tile_ids(int (&id)[CPT], const Geometry& g, const uint8_t* __r
     const int y = y0 + k.value * dy;
     id[k] = -1;
     if (z < g.nz && y < g.ny) {
-      id[k] = in_bulk_box(g, x, y, z)
-                ? kBoxCell
-                : int(ids[(uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z)]);
+      const int v = in_bulk_box(g, x, y, z)
+                      ? kBoxCell
+                      : int(ids[(uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z)]);
+      // a cell of the bulk entry collides like a box cell (the kernel
+      // argument holds that entry): no table loads
+      id[k] = v == g.bulk_id ? kBoxCell : v;
     }
   });
 }
