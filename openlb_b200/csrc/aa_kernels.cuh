@@ -213,6 +213,10 @@ struct StepVariant {
 #ifdef OLB_B200_SINGLE_VARIANT
 // builds that only check arithmetic compile one variant; every id maps to it
 constexpr StepVariant kStepVariants[] = {{1, 3}, {1, 3}, {1, 3}, {1, 3}};
+#elif defined(OLB_B200_EXACT)
+// the reference-order build serves parity, not speed: both work distributions
+// (one and two cells per thread), one register cap each
+constexpr StepVariant kStepVariants[] = {{1, 3}, {1, 3}, {2, 3}, {2, 3}};
 #else
 constexpr StepVariant kStepVariants[] = {{1, 3}, {1, 4}, {2, 2}, {2, 3}};
 #endif
@@ -410,9 +414,10 @@ OLB_DEV void load_tile_ids(int (&id)[CPT], const Geometry& g, const uint8_t* __r
   });
 }
 
-// Masked lattices: one tile per block, grid step_grid().  The ids of the
-// thread's cells are loaded first (none for cells of the bulk box); the
-// populations follow without waiting for them (step_tile).
+// Masked lattices: one tile per block, grid step_grid().  A warp inside the
+// bulk box runs the unmasked tile; any other warp loads its cells' ids first
+// (none for cells of the bulk box) and their populations without waiting for
+// them (step_tile).
 template <int Q, class S, class R, int KIND, bool ODD, bool STATS, int CPT, int MINB>
 __global__ void __launch_bounds__(kStepThreads, MINB)
 aa_step_masked_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict__ ids,
@@ -423,10 +428,22 @@ aa_step_masked_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __r
   const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
   const int x = blockIdx.z;
   const int dy = int(blockDim.y);
-  int id[CPT];
-  load_tile_ids(id, g, ids, x, y0, z, dy);
   StatAcc acc;
-  step_tile<Q, S, R, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, x, y0, z, dy, id, acc);
+  // a warp whose cells all lie in the bulk box takes the unmasked path (the
+  // branch is uniform across the warp); cells outside the lattice count as in
+  bool inside = true;
+  static_for<0, CPT>([&](auto k) {
+    const int y = y0 + k.value * dy;
+    inside = inside && (z >= g.nz || y >= g.ny || in_bulk_box(g, x, y, z));
+  });
+  if (__all_sync(0xffffffffu, inside)) {
+    const int none[CPT] = {};
+    step_tile<Q, S, R, KIND, ODD, false, STATS, CPT>(pops, g, nullptr, bulk, x, y0, z, dy, none, acc);
+  } else {
+    int id[CPT];
+    load_tile_ids(id, g, ids, x, y0, z, dy);
+    step_tile<Q, S, R, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, x, y0, z, dy, id, acc);
+  }
   if constexpr (STATS) {
     block_stats(acc.rho, acc.usqr, acc.max, acc.n, acc.nf, partials);
   }
@@ -763,11 +780,23 @@ aa_step_masked_paired_kernel(S* __restrict__ pops, const Geometry g, const uint8
   const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
   const int xp = blockIdx.z;
   const int dy = int(blockDim.y);
-  int lo[CPT], hi[CPT];
-  load_tile_ids(lo, g, ids, xp, y0, z, dy);
-  load_tile_ids(hi, g, ids, xp + (g.nx >> 1), y0, z, dy);
   StatAcc acc;
-  paired_tile<Q, S, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, xp, y0, z, dy, lo, hi, acc);
+  // both cells of every pair of the warp in the bulk box: the unmasked path
+  bool inside = true;
+  static_for<0, CPT>([&](auto k) {
+    const int y = y0 + k.value * dy;
+    inside = inside && (z >= g.nz || y >= g.ny ||
+                        (in_bulk_box(g, xp, y, z) && in_bulk_box(g, xp + (g.nx >> 1), y, z)));
+  });
+  if (__all_sync(0xffffffffu, inside)) {
+    const int none[CPT] = {};
+    paired_tile<Q, S, KIND, ODD, false, STATS, CPT>(pops, g, nullptr, bulk, xp, y0, z, dy, none, none, acc);
+  } else {
+    int lo[CPT], hi[CPT];
+    load_tile_ids(lo, g, ids, xp, y0, z, dy);
+    load_tile_ids(hi, g, ids, xp + (g.nx >> 1), y0, z, dy);
+    paired_tile<Q, S, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, xp, y0, z, dy, lo, hi, acc);
+  }
   if constexpr (STATS) {
     block_stats(acc.rho, acc.usqr, acc.max, acc.n, acc.nf, partials);
   }
