@@ -39,7 +39,6 @@ struct Geometry {
   // masked lattices: a box [lo, hi) whose cells all use the bulk entry, so the
   // step kernel skips their dynamics id (empty when lo == hi)
   int32_t bulk_lo[3], bulk_hi[3];
-  int32_t bulk_id;  // masked lattices: the table index of the bulk entry (-1: none)
   // FORCE per cell for the Guo-forced dynamics (3 columns of `stride` values
   // of the compute type, natural cell order), or nullptr: the entries' forces
   const void* force;
@@ -393,9 +392,8 @@ aa_step_kernel(S* __restrict__ pops, const Geometry g, const DynDevice<R> bulk, 
   }
 }
 
-// table entries of a tile's cells: kBoxCell for cells of the bulk box and
-// cells of the bulk entry (they use the kernel argument, no table load), -1 for
-// cells outside the lattice (skipped)
+// table entries of a tile's cells: kBoxCell for cells of the bulk box (they
+// use the bulk entry, no load), -1 for cells outside the lattice (skipped)
 template <int CPT>
 OLB_DEV void load_tile_ids(int (&id)[CPT], const Geometry& g, const uint8_t* __restrict__ ids, int x, int y0,
                            int z, int dy)
@@ -404,20 +402,16 @@ OLB_DEV void load_tile_ids(int (&id)[CPT], const Geometry& g, const uint8_t* __r
     const int y = y0 + k.value * dy;
     id[k] = -1;
     if (z < g.nz && y < g.ny) {
-      const int v = in_bulk_box(g, x, y, z)
-                      ? kBoxCell
-                      : int(ids[(uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z)]);
-      // a cell of the bulk entry collides like a box cell (the kernel
-      // argument holds that entry): no table loads
-      id[k] = v == g.bulk_id ? kBoxCell : v;
+      id[k] = in_bulk_box(g, x, y, z)
+                ? kBoxCell
+                : int(ids[(uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z)]);
     }
   });
 }
 
-// Masked lattices: one tile per block, grid step_grid().  A warp inside the
-// bulk box runs the unmasked tile; any other warp loads its cells' ids first
-// (none for cells of the bulk box) and their populations without waiting for
-// them (step_tile).
+// Masked lattices: one tile per block, grid step_grid().  The ids of the
+// thread's cells are loaded first (none for cells of the bulk box); the
+// populations follow without waiting for them (step_tile).
 template <int Q, class S, class R, int KIND, bool ODD, bool STATS, int CPT, int MINB>
 __global__ void __launch_bounds__(kStepThreads, MINB)
 aa_step_masked_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __restrict__ ids,
@@ -428,22 +422,10 @@ aa_step_masked_kernel(S* __restrict__ pops, const Geometry g, const uint8_t* __r
   const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
   const int x = blockIdx.z;
   const int dy = int(blockDim.y);
+  int id[CPT];
+  load_tile_ids(id, g, ids, x, y0, z, dy);
   StatAcc acc;
-  // a warp whose cells all lie in the bulk box takes the unmasked path (the
-  // branch is uniform across the warp); cells outside the lattice count as in
-  bool inside = true;
-  static_for<0, CPT>([&](auto k) {
-    const int y = y0 + k.value * dy;
-    inside = inside && (z >= g.nz || y >= g.ny || in_bulk_box(g, x, y, z));
-  });
-  if (__all_sync(0xffffffffu, inside)) {
-    const int none[CPT] = {};
-    step_tile<Q, S, R, KIND, ODD, false, STATS, CPT>(pops, g, nullptr, bulk, x, y0, z, dy, none, acc);
-  } else {
-    int id[CPT];
-    load_tile_ids(id, g, ids, x, y0, z, dy);
-    step_tile<Q, S, R, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, x, y0, z, dy, id, acc);
-  }
+  step_tile<Q, S, R, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, x, y0, z, dy, id, acc);
   if constexpr (STATS) {
     block_stats(acc.rho, acc.usqr, acc.max, acc.n, acc.nf, partials);
   }
@@ -593,6 +575,26 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
   bool go[CPT];
   uint32_t e[CPT];
 
+  // Odd step, a warp whose pairs all lie off every face and off the x seam:
+  // every neighbour is the element at a fixed offset (c_x ny nz + c_y nz + c_z)
+  // and no half swap is needed, so each population's address is e plus a
+  // constant that depends on the lattice only (uniform across the warp).
+  bool flat = false;
+  if constexpr (ODD) {
+    const int nxh = g.nx >> 1;
+    bool in = xp > 0 && xp < nxh - 1 && z > 0 && z < g.nz - 1;
+    static_for<0, CPT>([&](auto k) {
+      const int y = y0 + k.value * dy;
+      in = in && y > 0 && y < g.ny - 1;
+    });
+    flat = __all_sync(0xffffffffu, in);
+  }
+  const uint32_t sxy = uint32_t(g.ny) * uint32_t(g.nz);
+  // the element offset of lattice vector c (modulo 2^32: negative components wrap)
+  auto offset = [&](int cx, int cy, int cz) {
+    return uint32_t(cx) * sxy + uint32_t(cy) * uint32_t(g.nz) + uint32_t(cz);
+  };
+
   static_for<0, CPT>([&](auto k) {
     const int y = y0 + k.value * dy;
     go[k] = z < g.nz && y < g.ny;
@@ -608,6 +610,9 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
         // q * pstride < 2^32 (olb_b200_create)
         if constexpr (!ODD) {
           raw[k][i] = pops[uint32_t(i.value) * pstride + e[k]];
+        } else if (flat) {
+          constexpr int o = L::opp(i);
+          raw[k][i] = pops[e[k] + (uint32_t(o) * pstride - offset(L::c(i, 0), L::c(i, 1), L::c(i, 2)))];
         } else {
           constexpr int o = L::opp(i);
           const uint32_t src = nb.template at<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>();
@@ -740,6 +745,8 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
       if constexpr (!ODD) {
         constexpr int o = L::opp(i);
         pops[uint32_t(o) * ps + ek] = raw[k][i];
+      } else if (flat) {
+        pops[ek + (uint32_t(i.value) * ps + offset(L::c(i, 0), L::c(i, 1), L::c(i, 2)))] = raw[k][i];
       } else {
         const uint32_t dst = nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>();
         T v = raw[k][i];
@@ -780,23 +787,11 @@ aa_step_masked_paired_kernel(S* __restrict__ pops, const Geometry g, const uint8
   const int y0 = blockIdx.y * (blockDim.y * CPT) + threadIdx.y;
   const int xp = blockIdx.z;
   const int dy = int(blockDim.y);
+  int lo[CPT], hi[CPT];
+  load_tile_ids(lo, g, ids, xp, y0, z, dy);
+  load_tile_ids(hi, g, ids, xp + (g.nx >> 1), y0, z, dy);
   StatAcc acc;
-  // both cells of every pair of the warp in the bulk box: the unmasked path
-  bool inside = true;
-  static_for<0, CPT>([&](auto k) {
-    const int y = y0 + k.value * dy;
-    inside = inside && (z >= g.nz || y >= g.ny ||
-                        (in_bulk_box(g, xp, y, z) && in_bulk_box(g, xp + (g.nx >> 1), y, z)));
-  });
-  if (__all_sync(0xffffffffu, inside)) {
-    const int none[CPT] = {};
-    paired_tile<Q, S, KIND, ODD, false, STATS, CPT>(pops, g, nullptr, bulk, xp, y0, z, dy, none, none, acc);
-  } else {
-    int lo[CPT], hi[CPT];
-    load_tile_ids(lo, g, ids, xp, y0, z, dy);
-    load_tile_ids(hi, g, ids, xp + (g.nx >> 1), y0, z, dy);
-    paired_tile<Q, S, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, xp, y0, z, dy, lo, hi, acc);
-  }
+  paired_tile<Q, S, KIND, ODD, true, STATS, CPT>(pops, g, table, bulk, xp, y0, z, dy, lo, hi, acc);
   if constexpr (STATS) {
     block_stats(acc.rho, acc.usqr, acc.max, acc.n, acc.nf, partials);
   }

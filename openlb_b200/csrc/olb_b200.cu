@@ -371,7 +371,6 @@ void compute_bulk_box(olb_b200_lattice* L, const uint8_t* ids, int bulk_entry)
 {
   Geometry& g = L->g;
   for (int d = 0; d < 3; ++d) g.bulk_lo[d] = g.bulk_hi[d] = 0;
-  g.bulk_id = bulk_entry;
   if (!ids || bulk_entry < 0) return;
   const int n[3] = {L->desc.nx, L->desc.ny, L->desc.nz};
   auto id_at = [&](int x, int y, int z) { return int(ids[(size_t(x) * n[1] + y) * n[2] + z]); };
