@@ -575,26 +575,6 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
   bool go[CPT];
   uint32_t e[CPT];
 
-  // Odd step, a warp whose pairs all lie off every face and off the x seam:
-  // every neighbour is the element at a fixed offset (c_x ny nz + c_y nz + c_z)
-  // and no half swap is needed, so each population's address is e plus a
-  // constant that depends on the lattice only (uniform across the warp).
-  bool flat = false;
-  if constexpr (ODD) {
-    const int nxh = g.nx >> 1;
-    bool in = xp > 0 && xp < nxh - 1 && z > 0 && z < g.nz - 1;
-    static_for<0, CPT>([&](auto k) {
-      const int y = y0 + k.value * dy;
-      in = in && y > 0 && y < g.ny - 1;
-    });
-    flat = __all_sync(0xffffffffu, in);
-  }
-  const uint32_t sxy = uint32_t(g.ny) * uint32_t(g.nz);
-  // the element offset of lattice vector c (modulo 2^32: negative components wrap)
-  auto offset = [&](int cx, int cy, int cz) {
-    return uint32_t(cx) * sxy + uint32_t(cy) * uint32_t(g.nz) + uint32_t(cz);
-  };
-
   static_for<0, CPT>([&](auto k) {
     const int y = y0 + k.value * dy;
     go[k] = z < g.nz && y < g.ny;
@@ -610,9 +590,6 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
         // q * pstride < 2^32 (olb_b200_create)
         if constexpr (!ODD) {
           raw[k][i] = pops[uint32_t(i.value) * pstride + e[k]];
-        } else if (flat) {
-          constexpr int o = L::opp(i);
-          raw[k][i] = pops[e[k] + (uint32_t(o) * pstride - offset(L::c(i, 0), L::c(i, 1), L::c(i, 2)))];
         } else {
           constexpr int o = L::opp(i);
           const uint32_t src = nb.template at<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>();
@@ -745,8 +722,6 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
       if constexpr (!ODD) {
         constexpr int o = L::opp(i);
         pops[uint32_t(o) * ps + ek] = raw[k][i];
-      } else if (flat) {
-        pops[ek + (uint32_t(i.value) * ps + offset(L::c(i, 0), L::c(i, 1), L::c(i, 2)))] = raw[k][i];
       } else {
         const uint32_t dst = nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>();
         T v = raw[k][i];
