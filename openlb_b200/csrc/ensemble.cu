@@ -48,7 +48,7 @@ namespace {
 constexpr int kQ = 19;
 using L19 = Lattice<19>;
 constexpr int kEnsembleThreads = 256;
-constexpr int kTileCells = 2;  // cells per thread in a tile (their loads are in flight together)
+constexpr int kTileCells = 1;  // cells per thread in a tile
 constexpr int kTile = kEnsembleThreads * kTileCells;
 
 // q = floor(n / d) for n < 2^31 by one multiply-high, an add and a shift
@@ -145,93 +145,79 @@ ensemble_step_kernel(float* __restrict__ pool, const InstanceDevice* __restrict_
     float* __restrict__ pops = pool + I.pops;
     const uint32_t stride = I.stride;
     const Geometry g{I.nx, I.ny, I.nz, stride, 0};
-    const uint32_t nynz = I.nynz, nzu = I.nz_u;
-    // phase 1: every cell of the thread issues its loads before any collides
-    // (the populations go out with the cell's class, not after it: a wall
-    // cell's loads are wasted, its update being a no-op on the AA pattern)
-    float f[kTileCells][kQ];
-    int kind[kTileCells];
-    bool go[kTileCells], inner[kTileCells];
-    uint32_t n[kTileCells];
-    static_for<0, kTileCells>([&](auto k) {
-      n[k] = tile.start + threadIdx.x + uint32_t(k.value) * kEnsembleThreads;
-      go[k] = n[k] < I.cells;
-      kind[k] = CELL_WALL;
-      inner[k] = false;
-      if (!go[k]) return;
-      const uint32_t x = I.div_nynz.div(n[k]);
-      const uint32_t r = n[k] - x * I.nynz;
+#pragma unroll 1
+    for (int k = 0; k < kTileCells; ++k) {
+      const uint32_t n = tile.start + threadIdx.x + uint32_t(k) * kEnsembleThreads;
+      if (n >= I.cells) break;
+      const uint32_t x = I.div_nynz.div(n);
+      const uint32_t r = n - x * I.nynz;
       const uint32_t y = I.div_nz.div(r);
       const uint32_t z = r - y * I.nz_u;
-      kind[k] = cell_kind(pool, I, n[k], int(x), int(y), int(z));
+      const int kind = cell_kind(pool, I, n, int(x), int(y), int(z));
+      if (kind == CELL_WALL) continue;  // full-way bounce-back: AA no-op
       // Odd steps address neighbours.  A cell off every face of its box reaches
       // them without wrap-around: neighbour (x+cx, y+cy, z+cz) is the flat index
       // n + cx*ny*nz + cy*nz + cz, so each population's address is n plus a
       // per-instance constant.  Cells on a face (the lid row, the periodic x
       // ends of a channel) take the wrap-around offsets.
-      inner[k] = (x - 1u < uint32_t(I.nx - 2)) && (y - 1u < uint32_t(I.ny - 2)) && (z - 1u < uint32_t(I.nz - 2));
+      const bool inner = (x - 1u < uint32_t(I.nx - 2)) && (y - 1u < uint32_t(I.ny - 2)) &&
+                         (z - 1u < uint32_t(I.nz - 2));
+      const uint32_t nynz = I.nynz, nzu = I.nz_u;
+      float f[kQ];
       if (!odd) {
-        static_for<0, kQ>([&](auto i) { f[k][i] = pops[uint32_t(i.value) * stride + n[k]]; });
-      } else if (inner[k]) {
+        static_for<0, kQ>([&](auto i) { f[i] = pops[uint32_t(i.value) * stride + n]; });
+      } else if (inner) {
         static_for<0, kQ>([&](auto i) {
           constexpr int o = L::opp(i);
-          f[k][i] = pops[n[k] + (uint32_t(o) * stride + flat_offset<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>(nynz, nzu))];
+          f[i] = pops[n + (uint32_t(o) * stride +
+                           flat_offset<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>(nynz, nzu))];
         });
       } else {
         Neighbours nb(g, int(x), int(y), int(z));
         static_for<0, kQ>([&](auto i) {
           constexpr int o = L::opp(i);
-          f[k][i] = pops[uint32_t(o) * stride + nb.template at<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>()];
+          f[i] = pops[uint32_t(o) * stride + nb.template at<-L::c(i, 0), -L::c(i, 1), -L::c(i, 2)>()];
         });
       }
-    });
-    // phase 2: collide and store (walls store nothing: full-way bounce-back)
-    static_for<0, kTileCells>([&](auto k) {
-      if (!go[k] || kind[k] == CELL_WALL) return;
-      if (kind[k] == CELL_FLUID) {
+      if (kind == CELL_FLUID) {
         float rho, u[3];
         if (I.forced) {
           const float gg[3] = {I.force[0], I.force[1], I.force[2]};
           float delta;
-          compute_rho_delta_u_forced<L>(f[k], gg, rho, delta, u);
-          relax_bgk<L>(f[k], rho, delta, u, I.omega);
-          add_force<L>(f[k], rho, u, I.force_relax, gg);
+          compute_rho_delta_u_forced<L>(f, gg, rho, delta, u);
+          relax_bgk<L>(f, rho, delta, u, I.omega);
+          add_force<L>(f, rho, u, I.force_relax, gg);
         } else {
           float delta;
-          compute_rho_delta_u<L>(f[k], rho, delta, u);
-          relax_bgk<L>(f[k], rho, delta, u, I.omega);
+          compute_rho_delta_u<L>(f, rho, delta, u);
+          relax_bgk<L>(f, rho, delta, u, I.omega);
         }
       } else {
         // moving lid: collision::NguyenLaddCorrection<Revert>
-        revert<L>(f[k]);
+        revert<L>(f);
         static_for<1, kQ>([&](auto i) {
-          f[k][i] += I.lid_term[i][0];
-          f[k][i] += I.lid_term[i][1];
-          f[k][i] += I.lid_term[i][2];
+          f[i] += I.lid_term[i][0];
+          f[i] += I.lid_term[i][1];
+          f[i] += I.lid_term[i][2];
         });
       }
       const uint32_t st = opaque(stride);
-      const uint32_t nk = opaque(n[k]);
       if (!odd) {
         static_for<0, kQ>([&](auto i) {
           constexpr int o = L::opp(i);
-          pops[uint32_t(o) * st + nk] = f[k][i];
+          pops[uint32_t(o) * st + n] = f[i];
         });
-      } else if (inner[k]) {
+      } else if (inner) {
         static_for<0, kQ>([&](auto i) {
-          pops[nk + (uint32_t(i.value) * st + flat_offset<L::c(i, 0), L::c(i, 1), L::c(i, 2)>(nynz, nzu))] = f[k][i];
+          pops[n + (uint32_t(i.value) * st + flat_offset<L::c(i, 0), L::c(i, 1), L::c(i, 2)>(nynz, nzu))] = f[i];
         });
       } else {
-        // the cell's coordinates again (not kept live through the collision)
-        const uint32_t x = I.div_nynz.div(nk);
-        const uint32_t r = nk - x * I.nynz;
-        const uint32_t y = I.div_nz.div(r);
-        Neighbours nb(g, int(x), int(y), int(r - y * I.nz_u));
+        Neighbours nb(g, int(x), int(y), int(z));
         static_for<0, kQ>([&](auto i) {
-          pops[uint32_t(i.value) * st + nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>()] = f[k][i];
+          pops[uint32_t(i.value) * st + nb.template at<L::c(i, 0), L::c(i, 1), L::c(i, 2)>()] = f[i];
         });
       }
-    });
+    }
   }
 }
 
