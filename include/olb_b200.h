@@ -83,7 +83,13 @@ typedef enum {
    * PostStream stage (src/boundary/boundaryPostProcessors3D.hh:164-292);
    * `normal` holds the discrete normal. */
   OLB_B200_DYN_VELOCITY_EDGE = 11,        /* src/boundary/localVelocity3D.h:90-93,113-114 */
-  OLB_B200_DYN_VELOCITY_CORNER = 12       /* src/boundary/localVelocity3D.h:82-85,111-112 */
+  OLB_B200_DYN_VELOCITY_CORNER = 12,      /* src/boundary/localVelocity3D.h:82-85,111-112 */
+  /* Internal edges and corners of velocity boundaries (local and
+   * interpolated): CombinedRLBdynamics<MIXIN, momenta::InnerEdgeVelocityTuple3D
+   * / InnerCornerVelocityTuple3D> (src/dynamics/momenta/aliases.h:203-217), no
+   * post-processor; `normal` holds the discrete normal; BGK or TRT mixin. */
+  OLB_B200_DYN_VELOCITY_INNER_EDGE = 13,   /* src/boundary/localVelocity3D.h:98-101 */
+  OLB_B200_DYN_VELOCITY_INNER_CORNER = 14  /* src/boundary/localVelocity3D.h:88-91 */
 } olb_b200_dyn_kind;
 
 typedef struct {

@@ -9,7 +9,8 @@ from .descriptors import D3Q19, D3Q27, Descriptor, descriptor
 from .lattice import (BGKdynamics, BounceBack, BounceBackVelocity, Dynamics, ForcedBGKdynamics,
                       ForcedTRTdynamics, InterpolatedPressureBoundary, InterpolatedVelocityBoundary, Lattice,
                       LocalVelocityBoundary, NoDynamics, SmagorinskyBGKdynamics, SuperGeometry, SuperLattice,
-                      TRTdynamics, VelocityCornerBoundary, VelocityEdgeBoundary)
+                      TRTdynamics, VelocityCornerBoundary, VelocityEdgeBoundary, VelocityInnerCornerBoundary,
+                      VelocityInnerEdgeBoundary)
 
 OlbError = _abi.OlbError
 Diverged = _abi.Diverged
@@ -28,7 +29,8 @@ __all__ = [
     "D3Q19", "D3Q27", "Descriptor", "descriptor", "Dynamics", "NoDynamics", "BGKdynamics",
     "TRTdynamics", "ForcedTRTdynamics", "ForcedBGKdynamics", "SmagorinskyBGKdynamics", "BounceBack",
     "BounceBackVelocity", "InterpolatedVelocityBoundary", "InterpolatedPressureBoundary",
-    "LocalVelocityBoundary", "VelocityEdgeBoundary", "VelocityCornerBoundary", "boundary",
+    "LocalVelocityBoundary", "VelocityEdgeBoundary", "VelocityCornerBoundary", "VelocityInnerEdgeBoundary",
+    "VelocityInnerCornerBoundary", "boundary",
     "Lattice", "SuperGeometry", "SuperLattice", "OlbError", "Diverged",
     "LibraryNotBuilt", "library_path", "build_info",
 ]

@@ -909,6 +909,14 @@ __global__ void moments_kernel(const S* __restrict__ pops, const Geometry g, boo
     R f[Q];
     static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted); });
     bc_rho_u<L>(f, kind, p->bc_dir, p->bc_orient, p->bc_values + 4 * size_t(bc_index(p, x, y, z)), rho, u);
+  } else if (is_inner(kind)) {
+    // InnerEdge/CornerDensity3D + FixedVelocityMomentumGeneric
+    R f[Q];
+    static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted); });
+    const R* v = p->bc_values + 4 * size_t(bc_index(p, x, y, z));
+    u[0] = v[1]; u[1] = v[2]; u[2] = v[3];
+    const int32_t nn[3] = {p->nrm[0], p->nrm[1], p->nrm[2]};
+    rho = inner_rho<L>(f, kind, nn, u);
   } else if (is_outer(kind)) {
     // BulkDensity + FixedVelocityMomentumGeneric
     R f[Q];
@@ -1003,7 +1011,7 @@ OLB_DEV void cell_velocity(const S* __restrict__ pops, const Geometry& g, bool s
   } else if (is_interpolated(kind)) {
     const R* bu = e->bc_u + 3 * size_t(bc_index(e, p[0], p[1], p[2]));
     u[0] = bu[0]; u[1] = bu[1]; u[2] = bu[2];
-  } else if (kind == K_LOCAL_VELOCITY || is_outer(kind)) {
+  } else if (kind == K_LOCAL_VELOCITY || is_outer(kind) || is_inner(kind)) {
     // FixedVelocityMomentumGeneric: the VELOCITY field
     const R* v = e->bc_values + 4 * size_t(bc_index(e, p[0], p[1], p[2]));
     u[0] = v[1]; u[1] = v[2]; u[2] = v[3];
@@ -1041,6 +1049,12 @@ OLB_DEV R cell_density(const S* __restrict__ pops, const Geometry& g, bool shift
     bc_rho_u<L>(f, kind, e->bc_dir, e->bc_orient, e->bc_values + 4 * size_t(bc_index(e, p[0], p[1], p[2])), rho,
                 u);
     return rho;
+  }
+  if (is_inner(kind)) {
+    const R* v = e->bc_values + 4 * size_t(bc_index(e, p[0], p[1], p[2]));
+    const R u[3] = {v[1], v[2], v[3]};
+    const int32_t nn[3] = {e->nrm[0], e->nrm[1], e->nrm[2]};
+    return inner_rho<L>(f, kind, nn, u);
   }
   return compute_rho<L>(f);
 }

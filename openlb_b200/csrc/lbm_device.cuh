@@ -110,14 +110,19 @@ enum DynKind : int32_t {
   K_NONE = 0, K_BGK = 1, K_TRT = 2, K_SMAGORINSKY = 3, K_BOUNCE_BACK = 4,
   K_BOUNCE_BACK_VELOCITY = 5, K_FORCED_BGK = 6, K_FORCED_TRT = 7,
   K_INTERP_VELOCITY = 8, K_INTERP_PRESSURE = 9,
-  K_LOCAL_VELOCITY = 10, K_VELOCITY_EDGE = 11, K_VELOCITY_CORNER = 12
+  K_LOCAL_VELOCITY = 10, K_VELOCITY_EDGE = 11, K_VELOCITY_CORNER = 12,
+  K_VELOCITY_INNER_EDGE = 13, K_VELOCITY_INNER_CORNER = 14
 };
 
 OLB_HD bool is_interpolated(int kind) { return kind == K_INTERP_VELOCITY || kind == K_INTERP_PRESSURE; }
 // external edges and corners of velocity boundaries (OuterVelocity*Processor3D)
 OLB_HD bool is_outer(int kind) { return kind == K_VELOCITY_EDGE || kind == K_VELOCITY_CORNER; }
 // boundary cells whose values (RHO, VELOCITY) live in their entry's value box
-OLB_HD bool has_values(int kind) { return is_interpolated(kind) || kind == K_LOCAL_VELOCITY || is_outer(kind); }
+OLB_HD bool is_inner(int kind) { return kind == K_VELOCITY_INNER_EDGE || kind == K_VELOCITY_INNER_CORNER; }
+OLB_HD bool has_values(int kind)
+{
+  return is_interpolated(kind) || kind == K_LOCAL_VELOCITY || is_outer(kind) || is_inner(kind);
+}
 
 template <class R>
 struct DynDevice {
@@ -750,6 +755,106 @@ OLB_DEV void collide_local_velocity(R (&f)[L::q], const DynDevice<R>* __restrict
   st_usqr = norm_sqr(u);
 }
 
+// velocityBMRho<dir,orient>(cell, u)  src/dynamics/momenta/elements.h:54-71
+template <class L, class R>
+OLB_DEV R velocity_bm_rho(const R (&f)[L::q], int dir, int orient, const R (&u)[3])
+{
+  R on_wall, normal;
+  bc_sums<L>(f, dir, orient, on_wall, normal);
+  const R ud = dir == 0 ? u[0] : (dir == 1 ? u[1] : u[2]);
+  return (R(2) * normal + on_wall + R(1)) / (R(1) + R(orient) * ud);
+}
+
+// the two normal axes of an edge in the template order <plane, n[(plane+1)%3],
+// n[(plane+2)%3]> (src/boundary/setBoundary3D.h:156-197)
+OLB_DEV void edge_axes(const int32_t (&n)[3], int& d1, int& d2)
+{
+  const int plane = n[0] == 0 ? 0 : (n[1] == 0 ? 1 : 2);
+  d1 = plane == 2 ? 0 : plane + 1;
+  d2 = plane == 0 ? 2 : plane - 1;
+}
+
+// InnerEdgeDensity3D (src/dynamics/momenta/elements.h:427-438): the mean of
+// velocityBMRho along the edge's two normal axes; InnerCornerDensity3D
+// (:400-411): along all three
+template <class L, class R>
+OLB_DEV R inner_rho(const R (&f)[L::q], int kind, const int32_t (&n)[3], const R (&u)[3])
+{
+  if (kind == K_VELOCITY_INNER_CORNER) {
+    const R rx = velocity_bm_rho<L>(f, 0, n[0], u);
+    const R ry = velocity_bm_rho<L>(f, 1, n[1], u);
+    const R rz = velocity_bm_rho<L>(f, 2, n[2], u);
+    return (rx + ry + rz) / R(3);
+  }
+  int d1, d2;
+  edge_axes(n, d1, d2);
+  const R r1 = velocity_bm_rho<L>(f, d1, n[d1], u);
+  const R r2 = velocity_bm_rho<L>(f, d2, n[d2], u);
+  return (r1 + r2) / R(2);
+}
+
+// InnerEdgeStress3D (src/dynamics/momenta/elements.h:1739-1757): populations
+// arriving from both walls (c_i = -n on both normal axes) replaced by their
+// opposites' non-equilibrium parts; InnerCornerStress3D (:1711-1730): the one
+// population along -n (D3Q27 only); then lbm::computeStress (src/dynamics/lbm.h:311-329)
+template <class L, class R>
+OLB_DEV void inner_stress(const R (&f)[L::q], int kind, const int32_t (&n)[3], R rho, const R (&u)[3],
+                          R (&pi)[6])
+{
+  const R usqr = norm_sqr(u);
+  int d1 = 0, d2 = 1;
+  if (kind != K_VELOCITY_INNER_CORNER) edge_axes(n, d1, d2);
+  R g[L::q];
+  static_for<0, L::q>([&](auto i) {
+    constexpr int o = L::opp(i);
+    constexpr int c0 = L::c(i, 0), c1 = L::c(i, 1), c2 = L::c(i, 2);
+    const int ca = d1 == 0 ? c0 : (d1 == 1 ? c1 : c2);
+    const int cb = d2 == 0 ? c0 : (d2 == 1 ? c1 : c2);
+    const bool unknown = kind == K_VELOCITY_INNER_CORNER ? (c0 == -n[0] && c1 == -n[1] && c2 == -n[2])
+                                                          : (ca == -n[d1] && cb == -n[d2]);
+    g[i] = unknown ? f[o] - feq2<L, o>(rho, u, usqr) + feq2<L, i.value>(rho, u, usqr) : f[i];
+  });
+  static_for<0, 3>([&](auto a) {
+    static_for<a.value, 3>([&](auto b) {
+      constexpr int k = a.value * 3 - (a.value * (a.value - 1)) / 2 + (b.value - a.value);
+      R sum = R(0);
+      static_for<0, L::q>([&](auto i) { sum += R(L::c(i, a) * L::c(i, b)) * g[i]; });
+      sum -= rho * u[a] * u[b];
+      if constexpr (a.value == b.value) sum -= R(1) / R(3) * (rho - R(1));
+      pi[k] = sum;
+    });
+  });
+}
+
+// CombinedRLBdynamics<MIXIN, InnerEdgeVelocityTuple3D / InnerCornerVelocityTuple3D>
+// (src/boundary/localVelocity3D.h:88-101, interpolatedVelocity3D.h:56-67): as
+// collide_local_velocity with the inner density and stress
+template <class L, int KIND, class R>
+OLB_DEV void collide_inner_velocity(R (&f)[L::q], const DynDevice<R>* __restrict__ e, int x, int y, int z,
+                                    R& st_rho, R& st_usqr)
+{
+  const R* __restrict__ v = e->bc_values + 4 * size_t(bc_index(e, x, y, z));
+  const int kind = e->kind;
+  int32_t n[3] = {e->nrm[0], e->nrm[1], e->nrm[2]};
+  const R u[3] = {v[1], v[2], v[3]};
+  R pi[6];
+  R rho = inner_rho<L>(f, kind, n, u);
+  inner_stress<L>(f, kind, n, rho, u, pi);
+  {
+    const R usqr = norm_sqr(u);
+    static_for<0, L::q>([&](auto i) { f[i] = feq2<L, i.value>(rho, u, usqr) + from_pi_to_fneq<L, i.value>(pi); });
+  }
+  rho = inner_rho<L>(f, kind, n, u);
+  const R delta = rho - R(1);
+  if constexpr (KIND == K_TRT) {
+    relax_trt<L>(f, rho, delta, u, e->omega, e->omega_minus);
+  } else {
+    relax_bgk<L>(f, rho, delta, u, e->omega);
+  }
+  st_rho = rho;
+  st_usqr = norm_sqr(u);
+}
+
 // MIXIN::exchange_momenta<FixedVelocityBoundaryTuple> (src/dynamics/momenta/
 // aliases.h:188-193) on external edges and corners: BulkDensity and
 // u = VELOCITY; the mixin collision on those momenta.
@@ -785,6 +890,10 @@ OLB_DEV void collide_boundary(R (&f)[L::q], int kind, const DynDevice<R>* __rest
   } else if (kind == K_LOCAL_VELOCITY) {
     if constexpr (KIND == K_BGK || KIND == K_TRT) {
       collide_local_velocity<L, KIND>(f, e, x, y, z, st_rho, st_usqr);
+    }
+  } else if (is_inner(kind)) {
+    if constexpr (KIND == K_BGK || KIND == K_TRT) {
+      collide_inner_velocity<L, KIND>(f, e, x, y, z, st_rho, st_usqr);
     }
   } else {
     collide_fixed_velocity<L, KIND>(f, e, x, y, z, st_rho, st_usqr);

@@ -760,7 +760,7 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
   int bulk = -1, first_bc = -1;
   for (int k = 0; k < n_entries; ++k) {
     const int kind = table[k].kind;
-    if (kind < OLB_B200_DYN_NONE || kind > OLB_B200_DYN_VELOCITY_CORNER)
+    if (kind < OLB_B200_DYN_NONE || kind > OLB_B200_DYN_VELOCITY_INNER_CORNER)
       return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d has unknown kind %d", k, kind);
     if (table[k].reserved != 0)
       return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d: reserved field must be 0", k);
@@ -769,10 +769,10 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
       if (m != OLB_B200_DYN_BGK && m != OLB_B200_DYN_TRT && m != OLB_B200_DYN_SMAGORINSKY)
         return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: entry %d: boundaries take a BGK, TRT "
                     "or Smagorinsky-BGK mixin, got kind %d", k, m);
-      if (kind == OLB_B200_DYN_LOCAL_VELOCITY && m == OLB_B200_DYN_SMAGORINSKY)
-        return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: entry %d: local velocity boundaries with a "
-                    "Smagorinsky-BGK mixin are not implemented", k);
-      if (is_outer(kind)) {
+      if ((kind == OLB_B200_DYN_LOCAL_VELOCITY || is_inner(kind)) && m == OLB_B200_DYN_SMAGORINSKY)
+        return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: entry %d: regularised (local velocity, internal "
+                    "edge or corner) boundaries with a Smagorinsky-BGK mixin are not implemented", k);
+      if (is_outer(kind) || is_inner(kind)) {
         int nonzero = 0;
         bool valid = true;
         for (int e = 0; e < 3; ++e) {
@@ -780,10 +780,10 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
           valid &= v >= -1 && v <= 1;
           nonzero += v != 0;
         }
-        if (!valid || nonzero != (kind == OLB_B200_DYN_VELOCITY_EDGE ? 2 : 3))
+        const bool edge = kind == OLB_B200_DYN_VELOCITY_EDGE || kind == OLB_B200_DYN_VELOCITY_INNER_EDGE;
+        if (!valid || nonzero != (edge ? 2 : 3))
           return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d: normal (%d,%d,%d) is not an %s normal", k,
-                      table[k].normal[0], table[k].normal[1], table[k].normal[2],
-                      kind == OLB_B200_DYN_VELOCITY_EDGE ? "edge" : "corner");
+                      table[k].normal[0], table[k].normal[1], table[k].normal[2], edge ? "edge" : "corner");
       } else if (table[k].direction < 0 || table[k].direction > 2 ||
                  (table[k].orientation != 1 && table[k].orientation != -1)) {
         return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d: normal axis %d / sign %d invalid", k,

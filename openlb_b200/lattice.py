@@ -131,6 +131,20 @@ def VelocityCornerBoundary(mixin: Dynamics, normal) -> Dynamics:
                     smagorinsky=mixin.smagorinsky, mixin=mixin.kind, normal=tuple(int(v) for v in normal))
 
 
+def VelocityInnerEdgeBoundary(mixin: Dynamics, normal) -> Dynamics:
+    """Internal edge of a local or interpolated velocity boundary:
+    CombinedRLBdynamics of the mixin with InnerEdgeVelocityTuple3D momenta."""
+    return Dynamics(_abi.DYN_VELOCITY_INNER_EDGE, omega=mixin.omega, magic=mixin.magic,
+                    smagorinsky=mixin.smagorinsky, mixin=mixin.kind, normal=tuple(int(v) for v in normal))
+
+
+def VelocityInnerCornerBoundary(mixin: Dynamics, normal) -> Dynamics:
+    """Internal corner of a local or interpolated velocity boundary:
+    CombinedRLBdynamics of the mixin with InnerCornerVelocityTuple3D momenta."""
+    return Dynamics(_abi.DYN_VELOCITY_INNER_CORNER, omega=mixin.omega, magic=mixin.magic,
+                    smagorinsky=mixin.smagorinsky, mixin=mixin.kind, normal=tuple(int(v) for v in normal))
+
+
 FLUID_KINDS = {_abi.DYN_BGK, _abi.DYN_TRT, _abi.DYN_SMAGORINSKY, _abi.DYN_FORCED_BGK, _abi.DYN_FORCED_TRT}
 
 def splitmix64(x: np.ndarray) -> np.ndarray:

@@ -223,6 +223,70 @@ struct BoundaryValues<T,DESCRIPTOR,CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta:
   }
 };
 
+/// Internal edge of a local or interpolated velocity boundary
+/// (src/boundary/localVelocity3D.h:98-101, interpolatedVelocity3D.h:64-67):
+/// CombinedRLBdynamics<MIX, InnerEdgeVelocityTuple3D<plane,n1,n2>>; the discrete
+/// normal has n1 on axis (plane+1)%3 and n2 on axis (plane+2)%3
+/// (src/boundary/setBoundary3D.h:156-197)
+template <typename T, typename DESCRIPTOR, typename MIX, int plane, int n1, int n2>
+struct Describe<T,DESCRIPTOR,CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::InnerEdgeVelocityTuple3D<plane,n1,n2>>> {
+  using DYN = CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::InnerEdgeVelocityTuple3D<plane,n1,n2>>;
+  static constexpr int kind = Describe<T,DESCRIPTOR,MIX>::kind >= 0 ? OLB_B200_DYN_VELOCITY_INNER_EDGE : -1;
+  static constexpr bool perCell = false;
+  template <typename PARAMETERS>
+  static void shared(PARAMETERS& parameters, olb_b200_dyn_params& p)
+  {
+    mixinParameters<typename DYN::parameters>(parameters, p);
+    p.mixin = Describe<T,DESCRIPTOR,MIX>::kind;
+    p.normal[plane] = 0;
+    p.normal[(plane + 1) % 3] = n1;
+    p.normal[(plane + 2) % 3] = n2;
+  }
+  template <typename BLOCK>
+  static void cell(BLOCK&, CellID, olb_b200_dyn_params&) { }
+};
+
+template <typename T, typename DESCRIPTOR, typename MIX, int plane, int n1, int n2>
+struct BoundaryValues<T,DESCRIPTOR,CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::InnerEdgeVelocityTuple3D<plane,n1,n2>>> {
+  static constexpr bool valued = true;
+  template <typename BLOCK>
+  static void get(BLOCK& block, CellID iCell, double (&v)[4])
+  {
+    fixedVelocity(block, iCell, v);
+  }
+};
+
+/// Internal corner of a local or interpolated velocity boundary
+/// (src/boundary/localVelocity3D.h:88-91, interpolatedVelocity3D.h:56-59):
+/// CombinedRLBdynamics<MIX, InnerCornerVelocityTuple3D<nx,ny,nz>>
+template <typename T, typename DESCRIPTOR, typename MIX, int nx, int ny, int nz>
+struct Describe<T,DESCRIPTOR,CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::InnerCornerVelocityTuple3D<nx,ny,nz>>> {
+  using DYN = CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::InnerCornerVelocityTuple3D<nx,ny,nz>>;
+  static constexpr int kind = Describe<T,DESCRIPTOR,MIX>::kind >= 0 ? OLB_B200_DYN_VELOCITY_INNER_CORNER : -1;
+  static constexpr bool perCell = false;
+  template <typename PARAMETERS>
+  static void shared(PARAMETERS& parameters, olb_b200_dyn_params& p)
+  {
+    mixinParameters<typename DYN::parameters>(parameters, p);
+    p.mixin = Describe<T,DESCRIPTOR,MIX>::kind;
+    p.normal[0] = nx;
+    p.normal[1] = ny;
+    p.normal[2] = nz;
+  }
+  template <typename BLOCK>
+  static void cell(BLOCK&, CellID, olb_b200_dyn_params&) { }
+};
+
+template <typename T, typename DESCRIPTOR, typename MIX, int nx, int ny, int nz>
+struct BoundaryValues<T,DESCRIPTOR,CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::InnerCornerVelocityTuple3D<nx,ny,nz>>> {
+  static constexpr bool valued = true;
+  template <typename BLOCK>
+  static void get(BLOCK& block, CellID iCell, double (&v)[4])
+  {
+    fixedVelocity(block, iCell, v);
+  }
+};
+
 /// Interpolated velocity on a flat face (src/boundary/interpolatedVelocity3D.h:47-50):
 /// MIX::exchange_momenta<BasicDirichletVelocityBoundaryTuple<d,o>>
 template <typename T, typename DESCRIPTOR, typename EQ, typename COLL, typename COMB, int d, int o>

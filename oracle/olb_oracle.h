@@ -47,7 +47,13 @@ enum {
    * OuterVelocityEdgeProcessor3D (priority 0) / OuterVelocityCornerProcessor3D
    * (priority 1) after every stream; normal[] is the discrete normal */
   ORACLE_VELOCITY_EDGE = 11,       /* boundary/localVelocity3D.h:90-93,113-114; interpolatedVelocity3D.h:62-63,85-87 */
-  ORACLE_VELOCITY_CORNER = 12      /* boundary/localVelocity3D.h:82-85,111-112; interpolatedVelocity3D.h:54-55,81-83 */
+  ORACLE_VELOCITY_CORNER = 12,     /* boundary/localVelocity3D.h:82-85,111-112; interpolatedVelocity3D.h:54-55,81-83 */
+  /* internal edges and corners of velocity boundaries (local and
+   * interpolated): CombinedRLBdynamics<MIXIN, InnerEdgeVelocityTuple3D<plane,n1,n2>
+   * / InnerCornerVelocityTuple3D<nx,ny,nz>> (momenta/aliases.h:203-217), no
+   * post-processor; normal[] is the discrete normal */
+  ORACLE_VELOCITY_INNER_EDGE = 13,   /* boundary/localVelocity3D.h:98-101; interpolatedVelocity3D.h:64-67 */
+  ORACLE_VELOCITY_INNER_CORNER = 14  /* boundary/localVelocity3D.h:88-91; interpolatedVelocity3D.h:56-59 */
 };
 
 typedef struct {

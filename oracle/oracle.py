@@ -25,7 +25,8 @@ LIB_PATH = HERE / "_build" / "libolb_oracle.so"
 REF_DIR = HERE / "_ref"
 
 (NONE, BGK, TRT, SMAGORINSKY, BOUNCE_BACK, BOUNCE_BACK_VELOCITY, FORCED_BGK, FORCED_TRT,
- INTERP_VELOCITY, INTERP_PRESSURE, LOCAL_VELOCITY, VELOCITY_EDGE, VELOCITY_CORNER) = range(13)
+ INTERP_VELOCITY, INTERP_PRESSURE, LOCAL_VELOCITY, VELOCITY_EDGE, VELOCITY_CORNER,
+ VELOCITY_INNER_EDGE, VELOCITY_INNER_CORNER) = range(15)
 KIND_NAMES = {
     NONE: "none", BGK: "bgk", TRT: "trt", SMAGORINSKY: "smagorinsky",
     BOUNCE_BACK: "bounce_back", BOUNCE_BACK_VELOCITY: "bounce_back_velocity",
@@ -35,7 +36,10 @@ KIND_NAMES = {
 }
 INTERPOLATED = (INTERP_VELOCITY, INTERP_PRESSURE)
 # cells whose boundary values (RHO, VELOCITY) come from bc_values
-VALUED = (INTERP_VELOCITY, INTERP_PRESSURE, LOCAL_VELOCITY, VELOCITY_EDGE, VELOCITY_CORNER)
+VALUED = (INTERP_VELOCITY, INTERP_PRESSURE, LOCAL_VELOCITY, VELOCITY_EDGE, VELOCITY_CORNER,
+          VELOCITY_INNER_EDGE, VELOCITY_INNER_CORNER)
+# edge and corner entries: cells of their boundary setter's material
+SETTER_CELLS = (VELOCITY_EDGE, VELOCITY_CORNER, VELOCITY_INNER_EDGE, VELOCITY_INNER_CORNER)
 
 
 class _Dyn(ctypes.Structure):
@@ -275,7 +279,7 @@ def write_case(dirpath: Path, case: Case, steps: int, init: np.ndarray | None = 
         raise ValueError("the reference driver takes one lattice-wide OMEGA")
     for k, d in enumerate(case.table):
         # edge and corner entries are cells of their boundary setter's material
-        name = KIND_NAMES[d.boundary] if d.kind in (VELOCITY_EDGE, VELOCITY_CORNER) else KIND_NAMES[d.kind]
+        name = KIND_NAMES[d.boundary] if d.kind in SETTER_CELLS else KIND_NAMES[d.kind]
         lines.append(f"dyn {k + 1} {name}")
         if d.kind == BOUNCE_BACK_VELOCITY:
             lines.append("velocity {} {!r} {!r} {!r}".format(k + 1, *d.wall_u))

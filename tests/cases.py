@@ -181,8 +181,10 @@ def boundary_table(materials, normals, setters, bulk, mixin=O.BGK, velocity=None
                 key = (mat, typ, axis, nrm[axis])
                 entry = lambda a=axis, o=nrm[axis]: O.Dynamics(  # noqa: E731
                     setter, mixin=mixin, direction=a, orientation=o, **bulk)
-            elif typ in (EXTERNAL_EDGE, EXTERNAL_CORNER) and setter in (O.LOCAL_VELOCITY, O.INTERP_VELOCITY):
-                kind = O.VELOCITY_EDGE if typ == EXTERNAL_EDGE else O.VELOCITY_CORNER
+            elif typ in (EXTERNAL_EDGE, EXTERNAL_CORNER, INTERNAL_EDGE, INTERNAL_CORNER) and \
+                    setter in (O.LOCAL_VELOCITY, O.INTERP_VELOCITY):
+                kind = {EXTERNAL_EDGE: O.VELOCITY_EDGE, EXTERNAL_CORNER: O.VELOCITY_CORNER,
+                        INTERNAL_EDGE: O.VELOCITY_INNER_EDGE, INTERNAL_CORNER: O.VELOCITY_INNER_CORNER}[typ]
                 key = (mat, typ, nrm)
                 entry = lambda k=kind, v=nrm: O.Dynamics(  # noqa: E731
                     k, mixin=mixin, normal=v, boundary=setter, **bulk)
@@ -211,6 +213,30 @@ def local_velocity_cavity_case(q, size, omega=1 / 0.692, lid=(0.1, 0.0, 0.0), mi
     mats[:, -1, :] = 3
     normals = O.reference_normals(mats, (0, 0, 0), boundary_materials=(2, 3), q=q)
     ids, table, vals = boundary_table(mats, normals, {2: O.LOCAL_VELOCITY, 3: O.LOCAL_VELOCITY},
+                                      dict(omega=omega), mixin=mixin, velocity={3: lid})
+    return O.Case(q=q, size=size, periodic=(0, 0, 0), dyn_id=ids, table=table, bc_values=vals)
+
+
+def concave_cavity_case(q, size, omega=1 / 0.692, lid=(0.1, 0.0, 0.0), mixin=O.BGK, setter=O.LOCAL_VELOCITY):
+    """cavity3dBenchmark's default set-up with a block standing on the floor:
+    the block's surface is a velocity boundary too (u = 0), so OpenLB's
+    classification gives flat faces, external edges and corners (the box) and
+    internal edges and corners (where the block meets the floor, its top rim).
+    Wall cells that touch no fluid cell are bounce-back (material 4)."""
+    nx, ny, nz = size
+    mats = np.full(size, 2, np.int32)
+    mats[1:-1, 1:-1, 1:-1] = 1
+    mats[:, -1, :] = 3
+    mats[nx // 3:nx // 3 + 4, 1:5, nz // 3:nz // 3 + 4] = 2
+    fluid = mats == 1
+    near = np.zeros(size, bool)
+    for dx in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dz in (-1, 0, 1):
+                near |= np.roll(fluid, (dx, dy, dz), axis=(0, 1, 2))
+    mats[(mats == 2) & ~near] = 4
+    normals = O.reference_normals(mats, (0, 0, 0), boundary_materials=(2, 3), q=q)
+    ids, table, vals = boundary_table(mats, normals, {2: setter, 3: setter, 4: O.BOUNCE_BACK},
                                       dict(omega=omega), mixin=mixin, velocity={3: lid})
     return O.Case(q=q, size=size, periodic=(0, 0, 0), dyn_id=ids, table=table, bc_values=vals)
 

@@ -95,6 +95,17 @@ def fixture_cases():
         for variant in (("sisd", "nocse") if (q == 19 and dtype == np.float32) else ("sisd",)):
             name = f"open_inlet_q{q}_{np.dtype(dtype).name}_{O.KIND_NAMES[mixin]}_{variant}"
             out.append((name, case, f0, 15, dtype, variant, True))
+    # a block standing in cavity3dBenchmark's cavity: its surface adds the
+    # internal edges and corners of the velocity boundary (local and interpolated)
+    for q, dtype, setter, variants in ((19, np.float32, O.LOCAL_VELOCITY, ("sisd", "nocse")),
+                                       (19, np.float64, O.LOCAL_VELOCITY, ("sisd",)),
+                                       (27, np.float64, O.LOCAL_VELOCITY, ("sisd",)),
+                                       (19, np.float64, O.INTERP_VELOCITY, ("sisd",))):
+        case = C.concave_cavity_case(q, (12, 11, 10), setter=setter)
+        f0 = C.rest_state(q, case.n, dtype)
+        tag = "local" if setter == O.LOCAL_VELOCITY else "interp"
+        for variant in variants:
+            out.append((f"concave_{tag}_q{q}_{np.dtype(dtype).name}_{variant}", case, f0, 20, dtype, variant, True))
     # a FORCE value per cell (setField<FORCE> cell by cell) for the Guo-forced
     # dynamics: porous channel with forced TRT, periodic D3Q27 forced BGK
     frng = np.random.default_rng(31)

@@ -8,10 +8,14 @@ corners of velocity boundaries.
   boundaries): the mixin with FixedVelocityBoundaryTuple momenta plus
   OuterVelocityEdgeProcessor3D / OuterVelocityCornerProcessor3D in the
   PostStream stage (src/boundary/boundaryPostProcessors3D.hh:164-292).
+* Internal edges and corners (a block standing in the cavity):
+  CombinedRLBdynamics with InnerEdgeVelocityTuple3D / InnerCornerVelocityTuple3D
+  (src/dynamics/momenta/aliases.h:203-217, elements.h:400-438,1711-1757).
 
 Cases: cavity3dBenchmark's default set-up (the whole box surface LocalVelocity,
-the lid moving) and a channel whose whole inlet face, rim included, is an
-interpolated velocity inlet.  Discrete normals come from OpenLB's own
+the lid moving), a channel whose whole inlet face, rim included, is an
+interpolated velocity inlet, and the cavity with a block standing on its floor
+(local and interpolated).  Discrete normals come from OpenLB's own
 classification.
 
 Tolerances, relative to the unshifted population f_i: FP32 1e-5 against the
@@ -33,7 +37,8 @@ pytestmark = pytest.mark.gpu
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 FIXTURES = sorted(p.stem for p in GOLDEN.glob("local_cavity_*.npz")) + \
-    sorted(p.stem for p in GOLDEN.glob("open_inlet_*.npz"))
+    sorted(p.stem for p in GOLDEN.glob("open_inlet_*.npz")) + \
+    sorted(p.stem for p in GOLDEN.glob("concave_*.npz"))
 
 
 @pytest.mark.parametrize("name", FIXTURES)
@@ -53,7 +58,9 @@ def test_matches_reference_fixture(name):
 
 def _cases(q):
     return {"cavity": C.local_velocity_cavity_case(q, (20, 17, 15)),
-            "inlet": C.open_inlet_channel_case(q, (22, 12, 11), seed=3)}
+            "inlet": C.open_inlet_channel_case(q, (22, 12, 11), seed=3),
+            "concave": C.concave_cavity_case(q, (16, 13, 14)),
+            "concave_interp": C.concave_cavity_case(q, (15, 12, 13), setter=O.INTERP_VELOCITY)}
 
 
 @pytest.mark.parametrize("q", [19, 27])
