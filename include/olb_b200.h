@@ -89,7 +89,13 @@ typedef enum {
    * / InnerCornerVelocityTuple3D> (src/dynamics/momenta/aliases.h:203-217), no
    * post-processor; `normal` holds the discrete normal; BGK or TRT mixin. */
   OLB_B200_DYN_VELOCITY_INNER_EDGE = 13,   /* src/boundary/localVelocity3D.h:98-101 */
-  OLB_B200_DYN_VELOCITY_INNER_CORNER = 14  /* src/boundary/localVelocity3D.h:88-91 */
+  OLB_B200_DYN_VELOCITY_INNER_CORNER = 14, /* src/boundary/localVelocity3D.h:88-91 */
+  /* Local pressure boundary on a flat face: CombinedRLBdynamics<MIXIN,
+   * momenta::RegularizedPressureBoundaryTuple<direction,orientation>>
+   * (src/dynamics/momenta/aliases.h:136-141), no post-processor; BGK or TRT
+   * mixin.  The reference defines pressure boundaries on flat faces only
+   * (src/boundary/localPressure3D.h:47-57, interpolatedPressure3D.h:47-75). */
+  OLB_B200_DYN_LOCAL_PRESSURE = 15         /* boundary::LocalPressure (flat)  src/boundary/localPressure3D.h:47-57 */
 } olb_b200_dyn_kind;
 
 typedef struct {
@@ -109,10 +115,10 @@ typedef struct {
  *   force        descriptors::FORCE field value (Guo forcing, forcing.h:38-74)
  *   wall_u       descriptors::VELOCITY field of BounceBackVelocity (defineU)
  *   wall_rho     FixedDensity RHO field (1 unless defineRho)
- * Boundary entries (interpolated, local velocity, edges, corners) also carry
+ * Boundary entries (interpolated, local velocity or pressure, edges, corners) also carry
  *   mixin        the MixinDynamics template argument of the boundary setter
  *                (BGK, TRT or SMAGORINSKY; must be the lattice's fluid
- *                collision; local velocity faces take BGK or TRT)
+ *                collision; local faces, internal edges and corners take BGK or TRT)
  *   direction,   flat faces: the discrete normal as the boundary setter derives
  *   orientation  it (src/boundary/setBoundary3D.h:204-227): axis 0..2 and the
  *                sign of the outward normal, -1 or +1
@@ -166,7 +172,7 @@ void olb_b200_destroy(olb_b200_lattice* lattice);
 olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* lattice, const uint8_t* ids,
                                       const olb_b200_dyn_params* table, int32_t n_entries);
 
-/* Boundary values of interpolated boundary cells — replaces defineRho /
+/* Boundary values of the velocity and pressure boundary cells — replaces defineRho /
  * defineU on their cells (src/core/cell.h:194-198; FixedDensity RHO of
  * pressure cells, the VELOCITY field of FixedVelocityMomentumGeneric /
  * FixedPressureMomentum).  values[4*j .. 4*j+3] = RHO, VELOCITY x, y, z of

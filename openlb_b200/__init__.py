@@ -8,7 +8,7 @@ from . import _abi, boundary
 from .descriptors import D3Q19, D3Q27, Descriptor, descriptor
 from .lattice import (BGKdynamics, BounceBack, BounceBackVelocity, Dynamics, ForcedBGKdynamics,
                       ForcedTRTdynamics, InterpolatedPressureBoundary, InterpolatedVelocityBoundary, Lattice,
-                      LocalVelocityBoundary, NoDynamics, SmagorinskyBGKdynamics, SuperGeometry, SuperLattice,
+                      LocalPressureBoundary, LocalVelocityBoundary, NoDynamics, SmagorinskyBGKdynamics, SuperGeometry, SuperLattice,
                       TRTdynamics, VelocityCornerBoundary, VelocityEdgeBoundary, VelocityInnerCornerBoundary,
                       VelocityInnerEdgeBoundary)
 
@@ -29,7 +29,7 @@ __all__ = [
     "D3Q19", "D3Q27", "Descriptor", "descriptor", "Dynamics", "NoDynamics", "BGKdynamics",
     "TRTdynamics", "ForcedTRTdynamics", "ForcedBGKdynamics", "SmagorinskyBGKdynamics", "BounceBack",
     "BounceBackVelocity", "InterpolatedVelocityBoundary", "InterpolatedPressureBoundary",
-    "LocalVelocityBoundary", "VelocityEdgeBoundary", "VelocityCornerBoundary", "VelocityInnerEdgeBoundary",
+    "LocalVelocityBoundary", "LocalPressureBoundary", "VelocityEdgeBoundary", "VelocityCornerBoundary", "VelocityInnerEdgeBoundary",
     "VelocityInnerCornerBoundary", "boundary",
     "Lattice", "SuperGeometry", "SuperLattice", "OlbError", "Diverged",
     "LibraryNotBuilt", "library_path", "build_info",

@@ -32,11 +32,12 @@ STORAGE = {"f32": 0, "f64": 1, "f16": 2, "bf16": 3}
 DYN_NONE, DYN_BGK, DYN_TRT, DYN_SMAGORINSKY, DYN_BOUNCE_BACK, DYN_BOUNCE_BACK_VELOCITY, \
     DYN_FORCED_BGK, DYN_FORCED_TRT, DYN_INTERPOLATED_VELOCITY, DYN_INTERPOLATED_PRESSURE, \
     DYN_LOCAL_VELOCITY, DYN_VELOCITY_EDGE, DYN_VELOCITY_CORNER, DYN_VELOCITY_INNER_EDGE, \
-    DYN_VELOCITY_INNER_CORNER = range(15)
+    DYN_VELOCITY_INNER_CORNER, DYN_LOCAL_PRESSURE = range(16)
 DYN_INTERPOLATED = (DYN_INTERPOLATED_VELOCITY, DYN_INTERPOLATED_PRESSURE)
 # boundary kinds whose cells carry values (RHO, VELOCITY) set by set_boundary_values
 DYN_VALUED = (DYN_INTERPOLATED_VELOCITY, DYN_INTERPOLATED_PRESSURE, DYN_LOCAL_VELOCITY,
-              DYN_VELOCITY_EDGE, DYN_VELOCITY_CORNER, DYN_VELOCITY_INNER_EDGE, DYN_VELOCITY_INNER_CORNER)
+              DYN_VELOCITY_EDGE, DYN_VELOCITY_CORNER, DYN_VELOCITY_INNER_EDGE, DYN_VELOCITY_INNER_CORNER,
+              DYN_LOCAL_PRESSURE)
 ABI_VERSION = 3
 
 EXPORTED = [

@@ -1,14 +1,17 @@
-"""Boundary setters on the B200 platform: interpolated velocity / pressure.
+"""Boundary setters on the B200 platform: interpolated and local velocity /
+pressure boundaries.
 
 Mirrors ``boundary::set<boundary::InterpolatedVelocity>(sLattice, superGeometry,
-material)`` and ``...<InterpolatedPressure>`` (``src/boundary/setBoundary.h:79-157``):
-every cell of the material gets a discrete normal from the fluid cells
-(material 1) and the outside cells (material 0) around it
-(``computeBoundaryTypeAndNormal``, ``src/geometry/discreteNormals.hh:175-1191``),
-and from that its dynamics — the mixin collision with the boundary's momenta —
-and the ``PlaneFdBoundaryProcessor3D`` post-processor
-(``src/boundary/interpolatedVelocity3D.h:44-81``,
-``src/boundary/interpolatedPressure3D.h:47-90``).
+material)`` and ``...<InterpolatedPressure>``, ``<LocalVelocity>``,
+``<LocalPressure>`` (``src/boundary/setBoundary.h:79-157``): every cell of the
+material gets a discrete normal from the fluid cells (material 1) and the
+outside cells (material 0) around it (``computeBoundaryTypeAndNormal``,
+``src/geometry/discreteNormals.hh:175-1191``), and from that its dynamics — the
+mixin collision with the boundary's momenta and the ``PlaneFdBoundaryProcessor3D``
+post-processor (``src/boundary/interpolatedVelocity3D.h:44-81``,
+``src/boundary/interpolatedPressure3D.h:47-90``), or ``CombinedRLBdynamics``
+with regularised momenta and no post-processor
+(``src/boundary/localVelocity3D.h:47-80``, ``src/boundary/localPressure3D.h:47-57``).
 
 This build provides the flat-face type.  A boundary cell is flat when the four
 cells around it within one axis plane are neither fluid nor outside and a
@@ -29,6 +32,8 @@ FLAT = 0
 
 InterpolatedVelocity = _abi.DYN_INTERPOLATED_VELOCITY
 InterpolatedPressure = _abi.DYN_INTERPOLATED_PRESSURE
+LocalVelocity = _abi.DYN_LOCAL_VELOCITY
+LocalPressure = _abi.DYN_LOCAL_PRESSURE
 
 
 class UnsupportedBoundary(ValueError):
@@ -109,5 +114,5 @@ def set(lattice, geometry, material: int, kind: int = InterpolatedVelocity, mixi
     lattice.setBoundary(geometry, material, kind, mixin)
 
 
-__all__ = ["InterpolatedVelocity", "InterpolatedPressure", "UnsupportedBoundary", "discrete_normals",
-           "normal_groups", "padded_materials", "set"]
+__all__ = ["InterpolatedVelocity", "InterpolatedPressure", "LocalVelocity", "LocalPressure",
+           "UnsupportedBoundary", "discrete_normals", "normal_groups", "padded_materials", "set"]

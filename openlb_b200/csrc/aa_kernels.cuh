@@ -905,7 +905,7 @@ __global__ void moments_kernel(const S* __restrict__ pops, const Geometry g, boo
     rho = p->wall_rho; u[0] = u[1] = u[2] = R(0);
   } else if (kind == K_BOUNCE_BACK_VELOCITY) {
     rho = p->wall_rho; u[0] = p->wall_u[0]; u[1] = p->wall_u[1]; u[2] = p->wall_u[2];
-  } else if (is_interpolated(kind) || kind == K_LOCAL_VELOCITY) {
+  } else if (is_interpolated(kind) || is_local(kind)) {
     R f[Q];
     static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, x, y, z, shifted); });
     bc_rho_u<L>(f, kind, p->bc_dir, p->bc_orient, p->bc_values + 4 * size_t(bc_index(p, x, y, z)), rho, u);
@@ -1011,6 +1011,13 @@ OLB_DEV void cell_velocity(const S* __restrict__ pops, const Geometry& g, bool s
   } else if (is_interpolated(kind)) {
     const R* bu = e->bc_u + 3 * size_t(bc_index(e, p[0], p[1], p[2]));
     u[0] = bu[0]; u[1] = bu[1]; u[2] = bu[2];
+  } else if (kind == K_LOCAL_PRESSURE) {
+    // FixedPressureMomentum::computeU: VELOCITY, the normal part from the populations
+    R f[Q];
+    static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, p[0], p[1], p[2], shifted); });
+    R rho;
+    bc_rho_u<L>(f, kind, e->bc_dir, e->bc_orient, e->bc_values + 4 * size_t(bc_index(e, p[0], p[1], p[2])), rho,
+                u);
   } else if (kind == K_LOCAL_VELOCITY || is_outer(kind) || is_inner(kind)) {
     // FixedVelocityMomentumGeneric: the VELOCITY field
     const R* v = e->bc_values + 4 * size_t(bc_index(e, p[0], p[1], p[2]));
@@ -1044,7 +1051,7 @@ OLB_DEV R cell_density(const S* __restrict__ pops, const Geometry& g, bool shift
   if (kind == K_NONE) return R(1);
   R f[Q];
   static_for<0, Q>([&](auto i) { f[i] = logical_pop<Q, S, R, i.value>(pops, g, p[0], p[1], p[2], shifted); });
-  if (is_interpolated(kind) || kind == K_LOCAL_VELOCITY) {
+  if (is_interpolated(kind) || is_local(kind)) {
     R rho, u[3];
     bc_rho_u<L>(f, kind, e->bc_dir, e->bc_orient, e->bc_values + 4 * size_t(bc_index(e, p[0], p[1], p[2])), rho,
                 u);

@@ -111,17 +111,22 @@ enum DynKind : int32_t {
   K_BOUNCE_BACK_VELOCITY = 5, K_FORCED_BGK = 6, K_FORCED_TRT = 7,
   K_INTERP_VELOCITY = 8, K_INTERP_PRESSURE = 9,
   K_LOCAL_VELOCITY = 10, K_VELOCITY_EDGE = 11, K_VELOCITY_CORNER = 12,
-  K_VELOCITY_INNER_EDGE = 13, K_VELOCITY_INNER_CORNER = 14
+  K_VELOCITY_INNER_EDGE = 13, K_VELOCITY_INNER_CORNER = 14, K_LOCAL_PRESSURE = 15
 };
 
 OLB_HD bool is_interpolated(int kind) { return kind == K_INTERP_VELOCITY || kind == K_INTERP_PRESSURE; }
+// regularised flat faces (CombinedRLBdynamics with a Regularized*BoundaryTuple)
+OLB_HD bool is_local(int kind) { return kind == K_LOCAL_VELOCITY || kind == K_LOCAL_PRESSURE; }
+// faces whose density is fixed and whose normal velocity follows the populations
+OLB_HD bool is_pressure(int kind) { return kind == K_INTERP_PRESSURE || kind == K_LOCAL_PRESSURE; }
 // external edges and corners of velocity boundaries (OuterVelocity*Processor3D)
 OLB_HD bool is_outer(int kind) { return kind == K_VELOCITY_EDGE || kind == K_VELOCITY_CORNER; }
-// boundary cells whose values (RHO, VELOCITY) live in their entry's value box
+// internal edges and corners of velocity boundaries (InnerEdge/InnerCornerVelocityTuple3D)
 OLB_HD bool is_inner(int kind) { return kind == K_VELOCITY_INNER_EDGE || kind == K_VELOCITY_INNER_CORNER; }
+// boundary cells whose values (RHO, VELOCITY) live in their entry's value box
 OLB_HD bool has_values(int kind)
 {
-  return is_interpolated(kind) || kind == K_LOCAL_VELOCITY || is_outer(kind) || is_inner(kind);
+  return is_interpolated(kind) || is_local(kind) || is_outer(kind) || is_inner(kind);
 }
 
 template <class R>
@@ -626,7 +631,7 @@ OLB_DEV void bc_rho_u(const R (&f)[L::q], int kind, int dir, int orient, const R
   u[1] = v[2];
   u[2] = v[3];
   const R so = R(orient);
-  if (kind != K_INTERP_PRESSURE) {
+  if (!is_pressure(kind)) {
     const R ud = dir == 0 ? u[0] : (dir == 1 ? u[1] : u[2]);
     rho = (R(2) * normal + on_wall + R(1)) / (R(1) + so * ud);
   } else {
@@ -726,25 +731,27 @@ OLB_DEV void boundary_stress(const R (&f)[L::q], int dir, int orient, R rho, con
   });
 }
 
-// CombinedRLBdynamics<MIXIN, RegularizedVelocityBoundaryTuple<dir,orient>>::collide
-// (src/dynamics/dynamics.h:419-430): momenta rho = velocityBMRho, u = VELOCITY,
-// pi = the regularised boundary stress; the populations are rebuilt as
-// feq + fneq(pi), then the mixin collides with the same momenta evaluated
-// again on the rebuilt cell.
+// CombinedRLBdynamics<MIXIN, Regularized{Velocity,Pressure}BoundaryTuple<dir,orient>>
+// ::collide (src/dynamics/dynamics.h:419-430; tuples momenta/aliases.h:128-141):
+// momenta rho = velocityBMRho, u = VELOCITY (velocity faces) or rho = RHO,
+// u = VELOCITY with u[dir] from the populations (pressure faces,
+// FixedPressureMomentum::computeU, elements.h:594-616); pi = the regularised
+// boundary stress; the populations are rebuilt as feq + fneq(pi), then the
+// mixin collides with the same momenta evaluated again on the rebuilt cell.
 template <class L, int KIND, class R>
-OLB_DEV void collide_local_velocity(R (&f)[L::q], const DynDevice<R>* __restrict__ e, int x, int y, int z,
-                                    R& st_rho, R& st_usqr)
+OLB_DEV void collide_local(R (&f)[L::q], int kind, const DynDevice<R>* __restrict__ e, int x, int y, int z,
+                           R& st_rho, R& st_usqr)
 {
   const R* __restrict__ v = e->bc_values + 4 * size_t(bc_index(e, x, y, z));
   const int dir = e->bc_dir, orient = e->bc_orient;
   R rho, u[3], pi[6];
-  bc_rho_u<L>(f, K_LOCAL_VELOCITY, dir, orient, v, rho, u);
+  bc_rho_u<L>(f, kind, dir, orient, v, rho, u);
   boundary_stress<L>(f, dir, orient, rho, u, pi);
   {
     const R usqr = norm_sqr(u);
     static_for<0, L::q>([&](auto i) { f[i] = feq2<L, i.value>(rho, u, usqr) + from_pi_to_fneq<L, i.value>(pi); });
   }
-  bc_rho_u<L>(f, K_LOCAL_VELOCITY, dir, orient, v, rho, u);
+  bc_rho_u<L>(f, kind, dir, orient, v, rho, u);
   const R delta = rho - R(1);
   if constexpr (KIND == K_TRT) {
     relax_trt<L>(f, rho, delta, u, e->omega, e->omega_minus);
@@ -828,7 +835,7 @@ OLB_DEV void inner_stress(const R (&f)[L::q], int kind, const int32_t (&n)[3], R
 
 // CombinedRLBdynamics<MIXIN, InnerEdgeVelocityTuple3D / InnerCornerVelocityTuple3D>
 // (src/boundary/localVelocity3D.h:88-101, interpolatedVelocity3D.h:56-67): as
-// collide_local_velocity with the inner density and stress
+// collide_local with the inner density and stress
 template <class L, int KIND, class R>
 OLB_DEV void collide_inner_velocity(R (&f)[L::q], const DynDevice<R>* __restrict__ e, int x, int y, int z,
                                     R& st_rho, R& st_usqr)
@@ -887,9 +894,9 @@ OLB_DEV void collide_boundary(R (&f)[L::q], int kind, const DynDevice<R>* __rest
 {
   if (is_interpolated(kind)) {
     collide_interpolated<L, KIND>(f, kind, e, x, y, z, st_rho, st_usqr);
-  } else if (kind == K_LOCAL_VELOCITY) {
+  } else if (is_local(kind)) {
     if constexpr (KIND == K_BGK || KIND == K_TRT) {
-      collide_local_velocity<L, KIND>(f, e, x, y, z, st_rho, st_usqr);
+      collide_local<L, KIND>(f, kind, e, x, y, z, st_rho, st_usqr);
     }
   } else if (is_inner(kind)) {
     if constexpr (KIND == K_BGK || KIND == K_TRT) {

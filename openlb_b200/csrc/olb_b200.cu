@@ -523,8 +523,9 @@ olb_b200_status setup_boundaries(olb_b200_lattice* L, const uint8_t* ids, const 
   const int nx = L->desc.nx, ny = L->desc.ny, nz = L->desc.nz;
   std::vector<int> lo(size_t(n_entries) * 3, INT32_MAX), hi(size_t(n_entries) * 3, -1);
   // PostStream order: flat interpolated cells (velocity pass, PlaneFd), then
-  // external edges, then external corners; local velocity faces need no
-  // PostStream pass and come last (the boundary collision pre-pass takes all)
+  // external edges, then external corners; local faces and internal edges and
+  // corners need no PostStream pass and come last (the boundary collision
+  // pre-pass takes all)
   std::vector<uint32_t> flat, edges, corners, local;
   for (int x = 0; x < nx; ++x) {
     for (int y = 0; y < ny; ++y) {
@@ -760,7 +761,7 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
   int bulk = -1, first_bc = -1;
   for (int k = 0; k < n_entries; ++k) {
     const int kind = table[k].kind;
-    if (kind < OLB_B200_DYN_NONE || kind > OLB_B200_DYN_VELOCITY_INNER_CORNER)
+    if (kind < OLB_B200_DYN_NONE || kind > OLB_B200_DYN_LOCAL_PRESSURE)
       return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d has unknown kind %d", k, kind);
     if (table[k].reserved != 0)
       return fail(OLB_B200_ERR_ARG, "set_dynamics: entry %d: reserved field must be 0", k);
@@ -769,9 +770,9 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
       if (m != OLB_B200_DYN_BGK && m != OLB_B200_DYN_TRT && m != OLB_B200_DYN_SMAGORINSKY)
         return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: entry %d: boundaries take a BGK, TRT "
                     "or Smagorinsky-BGK mixin, got kind %d", k, m);
-      if ((kind == OLB_B200_DYN_LOCAL_VELOCITY || is_inner(kind)) && m == OLB_B200_DYN_SMAGORINSKY)
-        return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: entry %d: regularised (local velocity, internal "
-                    "edge or corner) boundaries with a Smagorinsky-BGK mixin are not implemented", k);
+      if ((is_local(kind) || is_inner(kind)) && m == OLB_B200_DYN_SMAGORINSKY)
+        return fail(OLB_B200_ERR_UNSUPPORTED, "set_dynamics: entry %d: regularised (local velocity or pressure, "
+                    "internal edge or corner) boundaries with a Smagorinsky-BGK mixin are not implemented", k);
       if (is_outer(kind) || is_inner(kind)) {
         int nonzero = 0;
         bool valid = true;

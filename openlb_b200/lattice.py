@@ -117,6 +117,15 @@ def LocalVelocityBoundary(mixin: Dynamics, direction: int, orientation: int) -> 
                     orientation=orientation)
 
 
+def LocalPressureBoundary(mixin: Dynamics, direction: int, orientation: int) -> Dynamics:
+    """boundary::LocalPressure on a flat face (src/boundary/localPressure3D.h:47-57):
+    CombinedRLBdynamics of the mixin with RegularizedPressureBoundaryTuple momenta
+    (src/dynamics/momenta/aliases.h:136-141)."""
+    return Dynamics(_abi.DYN_LOCAL_PRESSURE, omega=mixin.omega, magic=mixin.magic,
+                    smagorinsky=mixin.smagorinsky, mixin=mixin.kind, direction=direction,
+                    orientation=orientation)
+
+
 def VelocityEdgeBoundary(mixin: Dynamics, normal) -> Dynamics:
     """External edge of a local or interpolated velocity boundary: the mixin with
     FixedVelocityBoundaryTuple momenta plus OuterVelocityEdgeProcessor3D."""
@@ -144,6 +153,14 @@ def VelocityInnerCornerBoundary(mixin: Dynamics, normal) -> Dynamics:
     return Dynamics(_abi.DYN_VELOCITY_INNER_CORNER, omega=mixin.omega, magic=mixin.magic,
                     smagorinsky=mixin.smagorinsky, mixin=mixin.kind, normal=tuple(int(v) for v in normal))
 
+
+# the flat-face entry of each boundary setter the facade maps
+_FLAT_BOUNDARY = {
+    _abi.DYN_INTERPOLATED_VELOCITY: InterpolatedVelocityBoundary,
+    _abi.DYN_INTERPOLATED_PRESSURE: InterpolatedPressureBoundary,
+    _abi.DYN_LOCAL_VELOCITY: LocalVelocityBoundary,
+    _abi.DYN_LOCAL_PRESSURE: LocalPressureBoundary,
+}
 
 FLUID_KINDS = {_abi.DYN_BGK, _abi.DYN_TRT, _abi.DYN_SMAGORINSKY, _abi.DYN_FORCED_BGK, _abi.DYN_FORCED_TRT}
 
@@ -459,9 +476,10 @@ class SuperLattice:
         self._bc: dict[int, tuple] = {}          # material -> (kind, mixin Dynamics or None)
         self._bc_values = None                    # (4, n): RHO, VELOCITY of boundary cells
 
-    # boundary::set<InterpolatedVelocity / InterpolatedPressure>(sLattice, superGeometry, material)
+    # boundary::set<InterpolatedVelocity / InterpolatedPressure / LocalVelocity /
+    # LocalPressure>(sLattice, superGeometry, material)
     def setBoundary(self, geometry: SuperGeometry, material: int, kind: int, mixin: Dynamics | None = None) -> None:
-        if kind not in _abi.DYN_INTERPOLATED:
+        if kind not in _FLAT_BOUNDARY:
             raise ValueError(f"unknown boundary kind {kind}")
         self._bc[int(material)] = (kind, mixin)
 
@@ -548,7 +566,7 @@ class SuperLattice:
     def _table(self):
         table, ids = dynamics_table(self.geometry.materials, self._dyn_of_material, self._params,
                                     self._force, self._wall_u, self._wall_rho)
-        # interpolated boundaries: one entry per material and discrete normal
+        # flat boundaries: one entry per material and discrete normal
         from . import boundary
         for m, (kind, mixin) in sorted(self._bc.items()):
             mix = mixin if mixin is not None else BGKdynamics()
@@ -561,8 +579,7 @@ class SuperLattice:
                 kw["smagorinsky"] = self._params["SMAGORINSKY"]
             if kw:
                 mix = Dynamics(**{**mix.__dict__, **kw})
-            make = InterpolatedVelocityBoundary if kind == _abi.DYN_INTERPOLATED_VELOCITY else \
-                InterpolatedPressureBoundary
+            make = _FLAT_BOUNDARY[kind]
             for (axis, sign), cells in boundary.normal_groups(self.geometry.materials, self.geometry.periodic,
                                                               m).items():
                 if len(table) >= 256:

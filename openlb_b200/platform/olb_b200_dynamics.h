@@ -223,6 +223,40 @@ struct BoundaryValues<T,DESCRIPTOR,CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta:
   }
 };
 
+/// boundary::LocalPressure on a flat face (src/boundary/localPressure3D.h:47-57):
+/// CombinedRLBdynamics<MIX, RegularizedPressureBoundaryTuple<d,o>>
+template <typename T, typename DESCRIPTOR, typename MIX, int d, int o>
+struct Describe<T,DESCRIPTOR,CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::RegularizedPressureBoundaryTuple<d,o>>> {
+  using DYN = CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::RegularizedPressureBoundaryTuple<d,o>>;
+  static constexpr int kind = Describe<T,DESCRIPTOR,MIX>::kind >= 0 ? OLB_B200_DYN_LOCAL_PRESSURE : -1;
+  static constexpr bool perCell = false;
+  template <typename PARAMETERS>
+  static void shared(PARAMETERS& parameters, olb_b200_dyn_params& p)
+  {
+    mixinParameters<typename DYN::parameters>(parameters, p);
+    p.mixin = Describe<T,DESCRIPTOR,MIX>::kind;
+    p.direction = d;
+    p.orientation = o;
+  }
+  template <typename BLOCK>
+  static void cell(BLOCK&, CellID, olb_b200_dyn_params&) { }
+};
+
+template <typename T, typename DESCRIPTOR, typename MIX, int d, int o>
+struct BoundaryValues<T,DESCRIPTOR,CombinedRLBdynamics<T,DESCRIPTOR,MIX,momenta::RegularizedPressureBoundaryTuple<d,o>>> {
+  static constexpr bool valued = true;
+  template <typename BLOCK>
+  static void get(BLOCK& block, CellID iCell, double (&v)[4])
+  {
+    // FixedDensity RHO and the tangential velocity of FixedPressureMomentum<d,o>
+    v[0] = cellField<momenta::FixedDensity::RHO>(block, iCell, 1.0)[0];
+    const auto u = cellField<typename momenta::FixedPressureMomentum<d,o>::VELOCITY>(block, iCell, 0.0);
+    v[1] = u[0];
+    v[2] = u[1];
+    v[3] = u[2];
+  }
+};
+
 /// Internal edge of a local or interpolated velocity boundary
 /// (src/boundary/localVelocity3D.h:98-101, interpolatedVelocity3D.h:64-67):
 /// CombinedRLBdynamics<MIX, InnerEdgeVelocityTuple3D<plane,n1,n2>>; the discrete

@@ -53,7 +53,11 @@ enum {
    * / InnerCornerVelocityTuple3D<nx,ny,nz>> (momenta/aliases.h:203-217), no
    * post-processor; normal[] is the discrete normal */
   ORACLE_VELOCITY_INNER_EDGE = 13,   /* boundary/localVelocity3D.h:98-101; interpolatedVelocity3D.h:64-67 */
-  ORACLE_VELOCITY_INNER_CORNER = 14  /* boundary/localVelocity3D.h:88-91; interpolatedVelocity3D.h:56-59 */
+  ORACLE_VELOCITY_INNER_CORNER = 14, /* boundary/localVelocity3D.h:88-91; interpolatedVelocity3D.h:56-59 */
+  /* flat-face local pressure boundary: CombinedRLBdynamics<MIXIN,
+   * RegularizedPressureBoundaryTuple<direction,orientation>> (momenta/aliases.h:136-141),
+   * no post-processor */
+  ORACLE_LOCAL_PRESSURE = 15         /* boundary::LocalPressure (Flat)  boundary/localPressure3D.h:47-57 */
 };
 
 typedef struct {

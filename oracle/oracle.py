@@ -26,18 +26,18 @@ REF_DIR = HERE / "_ref"
 
 (NONE, BGK, TRT, SMAGORINSKY, BOUNCE_BACK, BOUNCE_BACK_VELOCITY, FORCED_BGK, FORCED_TRT,
  INTERP_VELOCITY, INTERP_PRESSURE, LOCAL_VELOCITY, VELOCITY_EDGE, VELOCITY_CORNER,
- VELOCITY_INNER_EDGE, VELOCITY_INNER_CORNER) = range(15)
+ VELOCITY_INNER_EDGE, VELOCITY_INNER_CORNER, LOCAL_PRESSURE) = range(16)
 KIND_NAMES = {
     NONE: "none", BGK: "bgk", TRT: "trt", SMAGORINSKY: "smagorinsky",
     BOUNCE_BACK: "bounce_back", BOUNCE_BACK_VELOCITY: "bounce_back_velocity",
     FORCED_BGK: "forced_bgk", FORCED_TRT: "forced_trt",
     INTERP_VELOCITY: "interpolated_velocity", INTERP_PRESSURE: "interpolated_pressure",
-    LOCAL_VELOCITY: "local_velocity",
+    LOCAL_VELOCITY: "local_velocity", LOCAL_PRESSURE: "local_pressure",
 }
 INTERPOLATED = (INTERP_VELOCITY, INTERP_PRESSURE)
 # cells whose boundary values (RHO, VELOCITY) come from bc_values
 VALUED = (INTERP_VELOCITY, INTERP_PRESSURE, LOCAL_VELOCITY, VELOCITY_EDGE, VELOCITY_CORNER,
-          VELOCITY_INNER_EDGE, VELOCITY_INNER_CORNER)
+          VELOCITY_INNER_EDGE, VELOCITY_INNER_CORNER, LOCAL_PRESSURE)
 # edge and corner entries: cells of their boundary setter's material
 SETTER_CELLS = (VELOCITY_EDGE, VELOCITY_CORNER, VELOCITY_INNER_EDGE, VELOCITY_INNER_CORNER)
 

@@ -32,10 +32,11 @@
  *                   `normals 2` stops after writing it)
  *
  * Interpolated boundaries (`dyn <m> interpolated_velocity|interpolated_pressure`)
- * and local velocity boundaries (`dyn <m> local_velocity`) are set like the
- * examples do, boundary::set<InterpolatedVelocity<T,D,MIXIN>> or
- * boundary::set<LocalVelocity<T,D,MIXIN>> (boundary/setBoundary.h:150-157,
- * boundary/interpolatedVelocity3D.h:36-98, boundary/localVelocity3D.h:36-120),
+ * and local boundaries (`dyn <m> local_velocity|local_pressure`) are set like the
+ * examples do, boundary::set<InterpolatedVelocity<T,D,MIXIN>>,
+ * boundary::set<LocalVelocity<T,D,MIXIN>> or boundary::set<LocalPressure<T,D,MIXIN>>
+ * (boundary/setBoundary.h:150-157, boundary/interpolatedVelocity3D.h:36-98,
+ * boundary/localVelocity3D.h:36-120, boundary/localPressure3D.h:36-66),
  * with the fluid material 1 and the outside material 0; MIXIN is the bulk
  * dynamics named by `bcmixin`.  Their boundary values go through Cell::defineRho
  * and Cell::defineU (core/cell.h:194-198).
@@ -162,7 +163,8 @@ void define(SuperLattice<T,DESCRIPTOR>& lattice, SuperGeometry<T,3>& geometry, i
 // per-cell boundary values through defineRho / defineU)
 bool is_interpolated(const std::string& kind)
 {
-  return kind == "interpolated_velocity" || kind == "interpolated_pressure" || kind == "local_velocity";
+  return kind == "interpolated_velocity" || kind == "interpolated_pressure" || kind == "local_velocity" ||
+         kind == "local_pressure";
 }
 
 template <typename MIXIN>
@@ -173,6 +175,8 @@ void set_interpolated(SuperLattice<T,DESCRIPTOR>& lattice, SuperGeometry<T,3>& g
     boundary::set<boundary::InterpolatedVelocity<T,DESCRIPTOR,MIXIN>>(lattice, geometry, m);
   } else if (kind == "local_velocity") {
     boundary::set<boundary::LocalVelocity<T,DESCRIPTOR,MIXIN>>(lattice, geometry, m);
+  } else if (kind == "local_pressure") {
+    boundary::set<boundary::LocalPressure<T,DESCRIPTOR,MIXIN>>(lattice, geometry, m);
   } else {
     boundary::set<boundary::InterpolatedPressure<T,DESCRIPTOR,MIXIN>>(lattice, geometry, m);
   }

@@ -142,6 +142,18 @@ def interpolated_channel_case(q, size, mixin=O.BGK, omega=1.6, smagorinsky=0.1, 
                   bc_values=vals.reshape(4, -1))
 
 
+def local_channel_case(q, size, mixin=O.BGK, omega=1.6, magic=3 / 16, u0=0.05, rho_out=0.995, side=0, seed=0):
+    """interpolated_channel_case with local boundaries, as resolvedRock3d and
+    microChannel3d set them: a LocalVelocity inlet on the x = 0 face and a
+    LocalPressure outlet (density rho_out) on the x = nx-1 face, both over the
+    interior y/z cells (flat faces only, the one type LocalPressure takes)."""
+    case = interpolated_channel_case(q, size, mixin=mixin, omega=omega, magic=magic, u0=u0, rho_out=rho_out,
+                                     side=side, seed=seed)
+    case.table[2].kind = O.LOCAL_VELOCITY
+    case.table[3].kind = O.LOCAL_PRESSURE
+    return case
+
+
 # DiscreteNormalType (src/geometry/discreteNormals.h:33-39)
 FLAT, EXTERNAL_CORNER, INTERNAL_CORNER, EXTERNAL_EDGE, INTERNAL_EDGE = range(5)
 

@@ -106,6 +106,16 @@ def fixture_cases():
         tag = "local" if setter == O.LOCAL_VELOCITY else "interp"
         for variant in variants:
             out.append((f"concave_{tag}_q{q}_{np.dtype(dtype).name}_{variant}", case, f0, 20, dtype, variant, True))
+    # LocalVelocity inlet and LocalPressure outlet (regularised flat faces)
+    for q, dtype, mixin, side, variants in ((19, np.float32, O.BGK, 0, ("sisd", "nocse")),
+                                            (19, np.float64, O.TRT, 2, ("sisd",)),
+                                            (27, np.float64, O.BGK, 2, ("sisd",)),
+                                            (27, np.float32, O.TRT, 0, ("sisd",))):
+        case = C.local_channel_case(q, (12, 8, 7), mixin=mixin, side=side, seed=q + side)
+        f0 = C.rest_state(q, case.n, dtype)
+        for variant in variants:
+            name = f"local_channel_q{q}_{np.dtype(dtype).name}_{O.KIND_NAMES[mixin]}_{variant}"
+            out.append((name, case, f0, 30, dtype, variant, True))
     # a FORCE value per cell (setField<FORCE> cell by cell) for the Guo-forced
     # dynamics: porous channel with forced TRT, periodic D3Q27 forced BGK
     frng = np.random.default_rng(31)

@@ -164,12 +164,18 @@ def test_mixin_must_match_fluid_collision():
         lat.close()
 
 
-def test_superlattice_facade_channel():
+@pytest.mark.parametrize("setters", ["interpolated", "local"])
+def test_superlattice_facade_channel(setters):
     """The OpenLB-style calls: materials, defineDynamics, boundary::set with
     discrete normals from the geometry, defineU / defineRho on the boundary
-    materials, initialize, collideAndStream — against the oracle."""
+    materials, initialize, collideAndStream — against the oracle; the inlet and
+    outlet set with InterpolatedVelocity / InterpolatedPressure or with
+    LocalVelocity / LocalPressure."""
     nx, ny, nz = 18, 10, 9
-    case = C.interpolated_channel_case(19, (nx, ny, nz), omega=1.4, seed=4)
+    make = C.interpolated_channel_case if setters == "interpolated" else C.local_channel_case
+    case = make(19, (nx, ny, nz), omega=1.4, seed=4)
+    inlet, outlet = (ob.boundary.InterpolatedVelocity, ob.boundary.InterpolatedPressure) \
+        if setters == "interpolated" else (ob.boundary.LocalVelocity, ob.boundary.LocalPressure)
     geo = ob.SuperGeometry((nx, ny, nz))
     mats = case.dyn_id.reshape(nx, ny, nz).astype(np.int32) + 1   # 1 fluid, 2 wall, 3 inlet, 4 outlet
     geo.materials[...] = mats
@@ -177,8 +183,8 @@ def test_superlattice_facade_channel():
     try:
         sl.defineDynamics(geo, 1, ob.BGKdynamics())
         sl.defineDynamics(geo, 2, ob.BounceBack())
-        ob.boundary.set(sl, geo, 3, ob.boundary.InterpolatedVelocity)
-        ob.boundary.set(sl, geo, 4, ob.boundary.InterpolatedPressure)
+        ob.boundary.set(sl, geo, 3, inlet)
+        ob.boundary.set(sl, geo, 4, outlet)
         sl.setParameter("OMEGA", 1.4)
         vals = case.bc_values.reshape(4, nx, ny, nz)
         sl.defineU(geo, 3, vals[1:])

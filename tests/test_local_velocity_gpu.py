@@ -1,9 +1,12 @@
-"""GPU parity of OpenLB's local velocity boundary and of the external edges and
-corners of velocity boundaries.
+"""GPU parity of OpenLB's local velocity and pressure boundaries and of the
+external and internal edges and corners of velocity boundaries.
 
 * boundary::LocalVelocity on flat faces: CombinedRLBdynamics with the
   regularised velocity-boundary momenta (src/boundary/localVelocity3D.h:47-80,
   src/dynamics/dynamics.h:394-437).
+* boundary::LocalPressure on flat faces: CombinedRLBdynamics with the
+  regularised pressure-boundary momenta (src/boundary/localPressure3D.h:47-57,
+  src/dynamics/momenta/aliases.h:136-141, elements.h:578-616).
 * External edges and corners (of local and of interpolated velocity
   boundaries): the mixin with FixedVelocityBoundaryTuple momenta plus
   OuterVelocityEdgeProcessor3D / OuterVelocityCornerProcessor3D in the
@@ -14,9 +17,10 @@ corners of velocity boundaries.
 
 Cases: cavity3dBenchmark's default set-up (the whole box surface LocalVelocity,
 the lid moving), a channel whose whole inlet face, rim included, is an
-interpolated velocity inlet, and the cavity with a block standing on its floor
-(local and interpolated).  Discrete normals come from OpenLB's own
-classification.
+interpolated velocity inlet, the cavity with a block standing on its floor
+(local and interpolated), and a channel with a LocalVelocity inlet and a
+LocalPressure outlet around a square cylinder.  Discrete normals come from
+OpenLB's own classification (the channels' faces are flat by construction).
 
 Tolerances, relative to the unshifted population f_i: FP32 1e-5 against the
 reference's own dumps and the oracle, FP64 1e-10 (fixtures) / 1e-12 (oracle);
@@ -38,7 +42,8 @@ pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).resolve().parent / "golden"
 FIXTURES = sorted(p.stem for p in GOLDEN.glob("local_cavity_*.npz")) + \
     sorted(p.stem for p in GOLDEN.glob("open_inlet_*.npz")) + \
-    sorted(p.stem for p in GOLDEN.glob("concave_*.npz"))
+    sorted(p.stem for p in GOLDEN.glob("concave_*.npz")) + \
+    sorted(p.stem for p in GOLDEN.glob("local_channel_*.npz"))
 
 
 @pytest.mark.parametrize("name", FIXTURES)
@@ -60,7 +65,8 @@ def _cases(q):
     return {"cavity": C.local_velocity_cavity_case(q, (20, 17, 15)),
             "inlet": C.open_inlet_channel_case(q, (22, 12, 11), seed=3),
             "concave": C.concave_cavity_case(q, (16, 13, 14)),
-            "concave_interp": C.concave_cavity_case(q, (15, 12, 13), setter=O.INTERP_VELOCITY)}
+            "concave_interp": C.concave_cavity_case(q, (15, 12, 13), setter=O.INTERP_VELOCITY),
+            "local_channel": C.local_channel_case(q, (22, 12, 11), side=2, seed=4)}
 
 
 @pytest.mark.parametrize("q", [19, 27])
@@ -90,8 +96,10 @@ def test_exact_build_is_bit_identical(q, storage):
             assert np.array_equal(got[valid], ref[valid]), (which, steps)
 
 
-def test_trt_mixin_matches_oracle():
-    case = C.local_velocity_cavity_case(19, (16, 14, 12), mixin=O.TRT)
+@pytest.mark.parametrize("which", ["cavity", "local_channel"])
+def test_trt_mixin_matches_oracle(which):
+    case = C.local_velocity_cavity_case(19, (16, 14, 12), mixin=O.TRT) if which == "cavity" else \
+        C.local_channel_case(19, (20, 11, 10), mixin=O.TRT, side=2, seed=9)
     f0 = C.rest_state(19, case.n, np.float32)
     ref = run_oracle(case, f0, 25)
     got, _, _ = run_gpu(case, f0, 25)

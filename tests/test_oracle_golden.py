@@ -130,4 +130,10 @@ def test_oracle_statistics_match_reference(name):
     rtol = 1e-6 if f.dtype == np.float32 else 1e-12
     np.testing.assert_allclose(st["sum_rho"] / n, avg_rho, rtol=rtol)
     np.testing.assert_allclose(0.5 * st["sum_usqr"] / n, avg_energy, rtol=max(rtol, 1e-5))
-    np.testing.assert_allclose(np.sqrt(st["max_usqr"]), max_u, rtol=rtol)
+    max_rtol = rtol
+    if name.startswith("local_channel_q19") and f.dtype == np.float32 and not expected_exact(name):
+        # max |u| sits on an outlet cell, whose normal velocity is
+        # (2 sum_normal + sum_wall + 1) / rho - 1: the CSE-reassociated sums of
+        # order 1 differ by an ulp or two (2.4e-7), 2e-6 of |u| ~ 0.13
+        max_rtol = 5e-6
+    np.testing.assert_allclose(np.sqrt(st["max_usqr"]), max_u, rtol=max_rtol)
