@@ -618,7 +618,7 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
     const int y = y0 + k.value * dy;
     // Both cells of the pair are collided in the scaled representation
     // g_i = s_i (f_i - w_i) of the storage, one after the other.  BGK and
-    // TRT cells collide on g directly (relax_*_scaled); any other dynamics
+    // TRT cells collide on g directly (relax_scaled); any other dynamics
     // decodes f_i = g_i / s_i, collides and re-encodes.  s_i of a population
     // equals that of its opposite, so the column read or written (i or
     // opp(i)) does not change the scale.

@@ -968,62 +968,70 @@ OLB_DEV void scaled_rho_u(const float (&g)[L::q], float& rho, float& delta, floa
   u[0] *= r; u[1] *= r; u[2] *= r;
 }
 
-// BGK (pair form) on g, with omega folded into the equilibrium terms:
-// g_i' = (1 - omega) g_i + A + B, g_opp' = (1 - omega) g_opp + A - B,
-// A = omega s t (delta + rho (9/2 (c.u)^2 - 3/2 |u|^2)), B = 3 omega s t rho (c.u)
-template <class L>
-OLB_DEV void relax_bgk_scaled(float (&g)[L::q], float rho, float delta, const float (&u)[3], float omega)
+// BGK / TRT relaxation on g in pair form, with the Guo force term folded in.
+// For a pair (i, opp) with sum s = g_i + g_opp and difference d = g_i - g_opp,
+//   TRT:  g_i' = S + D,  g_opp' = S - D,
+//         S = (1 - omega)/2 s + A,  D = (1 - omega_minus)/2 d + B
+//   BGK:  g_i' = (1 - omega) g_i + A + B,  g_opp' = (1 - omega) g_opp + A - B
+// with the equilibrium parts of A and B (per weight class k = s_i t_i):
+//   A = omega k (delta + rho (9/2 (c.u)^2 - 3/2 |u|^2)),  B = 3 omega' k rho (c.u)
+// (omega' = omega_minus for TRT, omega for BGK) and the Guo term of
+// lbm::addExternalForce (src/dynamics/lbm.h:544-566),
+//   t_i (3 (c_i - u).F + 9 (c_i.u)(c_i.F)) force_relax rho,
+// which over a pair is Fa +- Fb with Fa = k fr (9 (c.u)(c.F) - 3 u.F) and
+// Fb = 3 k fr (c.F), fr = force_relax rho: A += Fa, B += Fb.  Everything that
+// depends only on the weight class is formed once per class (the compiler
+// shares the products of equal constants), so a pair costs two dot products
+// with entries of +-1 and about a dozen FP32 operations.  The same collision
+// as relaxing and then adding the force (the rounding differs far below the
+// 16-bit storage's own).
+template <class L, bool TRT, bool FORCED>
+OLB_DEV void relax_scaled(float (&g)[L::q], float rho, float delta, const float (&u)[3], float usqr,
+                          float omega, float omega_minus, float force_relax, const float (&gf)[3])
 {
-  const float usqr = norm_sqr(u);
-  const float e0 = -1.5f * usqr;
-  const float keep = 1.f - omega;
-  const float omega_rho = omega * rho;
+  const float base = delta - 1.5f * rho * usqr;  // delta + rho e0
+  const float rho45 = 4.5f * rho;
+  const float rho_odd = (TRT ? omega_minus : omega) * rho;
+  float fr = 0.f, uf3 = 0.f;
+  if constexpr (FORCED) {
+    fr = force_relax * rho;
+    uf3 = 3.f * (u[0] * gf[0] + u[1] * gf[1] + u[2] * gf[2]);
+  }
   {
     constexpr float T = storage_scale<L>(0) * weight<L, float>(0);
-    const float wt = omega * T;
-    g[0] = keep * g[0] + wt * (delta + rho * e0);
+    float eq = (omega * T) * base;
+    if constexpr (FORCED) eq -= (T * fr) * uf3;
+    g[0] = fmaf(1.f - omega, g[0], eq);
   }
+  const float keep = TRT ? 0.5f * (1.f - omega) : 1.f - omega;
+  const float keep_minus = 0.5f * (1.f - omega_minus);
   static_for<1, L::half + 1>([&](auto i) {
     constexpr int o = L::opp(i);
     constexpr float T = storage_scale<L>(i) * weight<L, float>(i);
-    const float wt = omega * T;
-    const float cu = c_dot<L, i.value>(u);
-    const float ev = 4.5f * cu * cu + e0;
-    const float a = wt * (delta + rho * ev);
-    // 3 s_i w_i omega rho c.u with one rounded coefficient: its relative
-    // bias (the hi + lo split of the FP32 path) is far below the 16-bit
-    // storage rounding, so the split would only cost instructions here
     constexpr float K = 3.f * T;
-    const float b = K * (omega_rho * cu);
-    g[i] = (keep * g[i] + a) + b;
-    g[o] = (keep * g[o] + a) - b;
-  });
-}
-
-template <class L>
-OLB_DEV void relax_trt_scaled(float (&g)[L::q], float rho, float delta, const float (&u)[3], float omega,
-                              float omega_minus)
-{
-  const float usqr = norm_sqr(u);
-  const float e0 = -1.5f * usqr;
-  {
-    constexpr float T = storage_scale<L>(0) * weight<L, float>(0);
-    g[0] -= omega * (g[0] - T * (delta + rho * e0));
-  }
-  static_for<1, L::half + 1>([&](auto i) {
-    constexpr int o = L::opp(i);
-    constexpr float T = storage_scale<L>(i) * weight<L, float>(i);
+    const float wt = omega * T;
     const float cu = c_dot<L, i.value>(u);
-    const float ev = 4.5f * cu * cu + e0;
-    const float a = T * (delta + rho * ev);
-    constexpr float K = 3.f * T;  // one rounded coefficient (see relax_bgk_scaled)
-    const float b = K * (rho * cu);
-    const float dp = omega * (0.5f * (g[i] + g[o]) - a);
-    const float dm = omega_minus * (0.5f * (g[i] - g[o]) - b);
-    const float gi = g[i] - dp - dm;
-    const float go = g[o] - dp + dm;
-    g[i] = gi;
-    g[o] = go;
+    float a0 = wt * base;
+    float A, B;
+    if constexpr (FORCED) {
+      const float kf = T * fr;
+      a0 = fmaf(-kf, uf3, a0);
+      const float cf = c_dot<L, i.value>(gf);
+      A = fmaf(wt * rho45, cu * cu, fmaf(9.f * kf, cu * cf, a0));
+      B = fmaf(K * rho_odd, cu, (3.f * kf) * cf);
+    } else {
+      A = fmaf(wt * rho45, cu * cu, a0);
+      B = (K * rho_odd) * cu;
+    }
+    if constexpr (TRT) {
+      const float S = fmaf(keep, g[i] + g[o], A);
+      const float D = fmaf(keep_minus, g[i] - g[o], B);
+      g[i] = S + D;
+      g[o] = S - D;
+    } else {
+      g[i] = fmaf(keep, g[i], A + B);
+      g[o] = fmaf(keep, g[o], A - B);
+    }
   });
 }
 
@@ -1065,34 +1073,6 @@ OLB_DEV float smagorinsky_omega_scaled(const float (&g)[L::q], float rho, float 
   return 1.f / (tau_mol + tau_turb);
 }
 
-// Guo forcing (lbm::addExternalForce, src/dynamics/lbm.h:544-566) on g: the
-// term of population i, t_i (3 (c_i - u).F + 9 (c_i.u)(c_i.F)) force_relax rho,
-// scaled by s_i (folded into s_i t_i).  Over an opposite pair c_opp = -c_i the
-// two terms are A + B and A - B with A = 9 (c_i.u)(c_i.F) - 3 u.F and
-// B = 3 c_i.F, so each pair costs two dot products with entries of +-1.
-template <class L>
-OLB_DEV void add_force_scaled(float (&g)[L::q], float rho, const float (&u)[3], float force_relax,
-                              const float (&gf)[3])
-{
-  const float fr = force_relax * rho;
-  const float uf3 = 3.f * (u[0] * gf[0] + u[1] * gf[1] + u[2] * gf[2]);
-  {
-    constexpr float T = storage_scale<L>(0) * weight<L, float>(0);
-    g[0] -= uf3 * (T * fr);
-  }
-  static_for<1, L::half + 1>([&](auto i) {
-    constexpr int o = L::opp(i);
-    constexpr float T = storage_scale<L>(i) * weight<L, float>(i);
-    const float cu = c_dot<L, i.value>(u);
-    const float cf = c_dot<L, i.value>(gf);
-    const float a = 9.f * cu * cf - uf3;
-    const float b = 3.f * cf;
-    const float k = T * fr;
-    g[i] += (a + b) * k;
-    g[o] += (a - b) * k;
-  });
-}
-
 // Any fluid collision on the scaled 16-bit representation (see above).
 template <class L, int KIND>
 OLB_DEV void collide_scaled(float (&g)[L::q], const DynDevice<float>& p, float& st_rho, float& st_usqr)
@@ -1105,19 +1085,17 @@ OLB_DEV void collide_scaled(float (&g)[L::q], const DynDevice<float>& p, float& 
     gf[0] = p.force[0]; gf[1] = p.force[1]; gf[2] = p.force[2];
     u[0] += gf[0] * 0.5f; u[1] += gf[1] * 0.5f; u[2] += gf[2] * 0.5f;
   }
+  const float usqr = norm_sqr(u);
   if constexpr (KIND == K_TRT || KIND == K_FORCED_TRT) {
-    relax_trt_scaled<L>(g, rho, delta, u, p.omega, p.omega_minus);
+    relax_scaled<L, true, forced>(g, rho, delta, u, usqr, p.omega, p.omega_minus, p.force_relax, gf);
   } else if constexpr (KIND == K_SMAGORINSKY) {
     const float w = smagorinsky_omega_scaled<L>(g, rho, delta, u, p.smago_pre, p.tau_mol);
-    relax_bgk_scaled<L>(g, rho, delta, u, w);
+    relax_scaled<L, false, false>(g, rho, delta, u, usqr, w, w, 0.f, gf);
   } else {
-    relax_bgk_scaled<L>(g, rho, delta, u, p.omega);
-  }
-  if constexpr (forced) {
-    add_force_scaled<L>(g, rho, u, p.force_relax, gf);
+    relax_scaled<L, false, forced>(g, rho, delta, u, usqr, p.omega, p.omega, p.force_relax, gf);
   }
   st_rho = rho;
-  st_usqr = norm_sqr(u);
+  st_usqr = usqr;
 }
 
 // collision::NguyenLaddCorrection<Revert>  src/dynamics/collision.h:333-346
