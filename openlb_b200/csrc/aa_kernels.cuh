@@ -42,6 +42,10 @@ struct Geometry {
   // FORCE per cell for the Guo-forced dynamics (3 columns of `stride` values
   // of the compute type, natural cell order), or nullptr: the entries' forces
   const void* force;
+  // masked lattices: 1 when every entry of the bulk entry's collision kind has
+  // the bulk entry's constants, so the step kernel takes them from the kernel
+  // argument instead of loading them from the cell's table entry
+  int32_t uniform;
 };
 
 // the entry index the masked kernels give a cell of the bulk box (the table
@@ -300,7 +304,7 @@ OLB_DEV void step_tile(S* __restrict__ pops, const Geometry& g, const DynDevice<
       if constexpr (MASKED) {
         // the entry's collision constants (the bulk entry's for box cells)
         DynDevice<R> q;
-        if (id[k] == kBoxCell) {
+        if (id[k] == kBoxCell || g.uniform) {
           q.omega = bulk.omega;
           q.omega_minus = bulk.omega_minus;
           q.smago_pre = bulk.smago_pre;
@@ -448,12 +452,74 @@ template <> struct Pair<__half> {
   using T = __half2;
   OLB_DEV static float2 to_float2(T v) { return __half22float2(v); }
   OLB_DEV static T from_floats(float lo, float hi) { return __floats2half2_rn(lo, hi); }
+  OLB_DEV static T from_float2(float2 v) { return __float22half2_rn(v); }
 };
 template <> struct Pair<__nv_bfloat16> {
   using T = __nv_bfloat162;
   OLB_DEV static float2 to_float2(T v) { return __bfloat1622float2(v); }
   OLB_DEV static T from_floats(float lo, float hi) { return __floats2bfloat162_rn(lo, hi); }
+  OLB_DEV static T from_float2(float2 v) { return __float22bfloat162_rn(v); }
 };
+
+// the fluid collision constants of a cell for the scaled collisions (KIND the
+// lattice's fluid kind): its table entry's when `own` and it has one, else the
+// bulk entry's (kernel argument); `wall`: the constants that make the same
+// arithmetic a full-way bounce-back (see ScaledParams)
+template <int KIND>
+OLB_DEV ScaledParams<float> scaled_params(const DynDevice<float>* pe, bool own, const DynDevice<float>& bulk,
+                                          bool wall = false)
+{
+  ScaledParams<float> q;
+  if (own && pe) {
+    q.omega = __ldg(&pe->omega);
+    q.omega_b = __ldg(&pe->omega_minus);
+    q.smago_pre = __ldg(&pe->smago_pre);
+    q.tau_mol = __ldg(&pe->tau_mol);
+    q.force_relax = __ldg(&pe->force_relax);
+    q.force[0] = __ldg(&pe->force[0]);
+    q.force[1] = __ldg(&pe->force[1]);
+    q.force[2] = __ldg(&pe->force[2]);
+  } else {
+    q.omega = bulk.omega;
+    q.omega_b = bulk.omega_minus;
+    q.smago_pre = bulk.smago_pre;
+    q.tau_mol = bulk.tau_mol;
+    q.force_relax = bulk.force_relax;
+    q.force[0] = bulk.force[0];
+    q.force[1] = bulk.force[1];
+    q.force[2] = bulk.force[2];
+  }
+  if (!(KIND == K_TRT || KIND == K_FORCED_TRT)) q.omega_b = q.omega;
+  q.keep = 0.5f * (1.f - q.omega);
+  q.keep_minus = 0.5f * (1.f - q.omega_b);
+  q.live = 1.f;
+  if (wall) {
+    q.omega = q.omega_b = q.force_relax = 0.f;
+    q.force[0] = q.force[1] = q.force[2] = 0.f;
+    q.keep = 0.5f;
+    q.keep_minus = -0.5f;
+    q.live = 0.f;
+  }
+  return q;
+}
+
+// the constants of two cells as the lanes of one pair
+OLB_DEV ScaledParams<float2> zip_params(const ScaledParams<float>& a, const ScaledParams<float>& b)
+{
+  ScaledParams<float2> q;
+  q.omega = make_float2(a.omega, b.omega);
+  q.omega_b = make_float2(a.omega_b, b.omega_b);
+  q.keep = make_float2(a.keep, b.keep);
+  q.keep_minus = make_float2(a.keep_minus, b.keep_minus);
+  q.smago_pre = make_float2(a.smago_pre, b.smago_pre);
+  q.tau_mol = make_float2(a.tau_mol, b.tau_mol);
+  q.live = make_float2(a.live, b.live);
+  q.force_relax = make_float2(a.force_relax, b.force_relax);
+  q.force[0] = make_float2(a.force[0], b.force[0]);
+  q.force[1] = make_float2(a.force[1], b.force[1]);
+  q.force[2] = make_float2(a.force[2], b.force[2]);
+  return q;
+}
 
 // byte permutation of a packed pair (one PRMT): 0x3210 keeps it, 0x1032 swaps
 // the halves; pair_merge_lo/hi take the low/high halves of a and b
@@ -498,13 +564,14 @@ struct PairNeighbours {
 // field: the Guo-forced dynamics take the cell's FORCE from fcell
 template <class L, int KIND, bool MASKED>
 OLB_DEV bool collide_any(float (&f)[L::q], int kind, const DynDevice<float>* e, const DynDevice<float>& bulk,
-                         const float (&fcell)[3], bool field, float& st_rho, float& st_usqr)
+                         const float (&fcell)[3], bool field, bool uniform, float& st_rho, float& st_usqr)
 {
   constexpr bool kForced = KIND == K_FORCED_BGK || KIND == K_FORCED_TRT;
   if (kind == KIND) {
-    if ((MASKED && e) || (kForced && field)) {
+    const bool own = MASKED && e && !uniform;  // the entry's constants, not the bulk entry's
+    if (own || (kForced && field)) {
       DynDevice<float> q;
-      if (MASKED && e) {
+      if (own) {
         q.omega = __ldg(&e->omega);
         q.omega_minus = __ldg(&e->omega_minus);
         q.smago_pre = __ldg(&e->smago_pre);
@@ -616,12 +683,60 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
   static_for<0, CPT>([&](auto k) {
     if (!go[k]) return;
     const int y = y0 + k.value * dy;
-    // Both cells of the pair are collided in the scaled representation
-    // g_i = s_i (f_i - w_i) of the storage, one after the other.  BGK and
-    // TRT cells collide on g directly (relax_scaled); any other dynamics
-    // decodes f_i = g_i / s_i, collides and re-encodes.  s_i of a population
-    // equals that of its opposite, so the column read or written (i or
-    // opp(i)) does not change the scale.
+    // the table entries (nullptr: the bulk entry, the kernel argument)
+    const DynDevice<float>* pe_lo = MASKED && id_lo[k] != kBoxCell ? table + id_lo[k] : nullptr;
+    const DynDevice<float>* pe_hi = MASKED && id_hi[k] != kBoxCell ? table + id_hi[k] : nullptr;
+    const bool field = kForced && g.force != nullptr;
+    // the cell's FORCE when the lattice has a force field (Guo-forced
+    // dynamics; loaded here, after the populations)
+    auto load_force = [&](int x, float (&fc)[3]) {
+      const float* __restrict__ F = static_cast<const float*>(g.force);
+      const uint32_t nn = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
+      fc[0] = __ldg(F + nn);
+      fc[1] = __ldg(F + size_t(g.stride) + nn);
+      fc[2] = __ldg(F + 2 * size_t(g.stride) + nn);
+    };
+#ifndef OLB_B200_EXACT
+    // both cells collide with the lattice's fluid kind, or one of them is a
+    // full-way bounce-back wall (a pair of two walls stores nothing)
+    bool both = true;
+    bool wall_lo = false, wall_hi = false;
+    if constexpr (MASKED) {
+      wall_lo = kind_lo[k] == K_BOUNCE_BACK;
+      wall_hi = kind_hi[k] == K_BOUNCE_BACK;
+      both = (kind_lo[k] == KIND || wall_lo) && (kind_hi[k] == KIND || wall_hi);
+    }
+    if (both) {
+      // Both cells at once, in the scaled representation g_i = s_i (f_i - w_i)
+      // of the storage: lane x the low cell, lane y the high one, straight
+      // from and back to the packed pairs (packed FP32 arithmetic); a wall
+      // lane takes the constants that make the collision a bounce-back.
+      float2 g2[Q];
+      static_for<0, Q>([&](auto i) { g2[i] = P::to_float2(raw[k][i]); });
+      ScaledParams<float> lo = scaled_params<KIND>(pe_lo, MASKED && !g.uniform, bulk, wall_lo);
+      ScaledParams<float> hi = scaled_params<KIND>(pe_hi, MASKED && !g.uniform, bulk, wall_hi);
+      if constexpr (kForced) {
+        if (field) {
+          if (!wall_lo) load_force(xp, lo.force);
+          if (!wall_hi) load_force(xp + (g.nx >> 1), hi.force);
+        }
+      }
+      const ScaledParams<float2> q2 = zip_params(lo, hi);
+      float2 r2, u22;
+      collide_scaled<L, KIND>(g2, q2, r2, u22);
+      static_for<0, Q>([&](auto i) { raw[k][i] = P::from_float2(g2[i]); });
+      if constexpr (STATS) {
+        if (!wall_lo) acc.add(double(r2.x), double(u22.x));
+        if (!wall_hi) acc.add(double(r2.y), double(u22.y));
+      }
+    } else
+#endif
+    {
+    // One cell after the other (a pair with a wall or boundary cell, and the
+    // exact build).  BGK and TRT cells collide on g directly (collide_scaled);
+    // any other dynamics decodes f_i = g_i / s_i, collides and re-encodes.
+    // s_i of a population equals that of its opposite, so the column read or
+    // written (i or opp(i)) does not change the scale.
     // the low cell's results wait in packed pairs of populations (half the
     // registers); the high cell's are packed the same way and the two are
     // merged with one byte permutation per population
@@ -637,46 +752,17 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
       });
       float r = 0.f, u2 = 0.f;
       bool counted = false, done = false;
-      // the cell's FORCE when the lattice has a force field (Guo-forced
-      // dynamics; loaded here, after the populations)
       float fcell[3] = {0.f, 0.f, 0.f};
-      const bool field = kForced && g.force != nullptr;
       if constexpr (kForced) {
-        if (field && (!MASKED || kind == KIND)) {
-          const float* __restrict__ F = static_cast<const float*>(g.force);
-          const uint32_t nn = (uint32_t(x) * uint32_t(g.ny) + uint32_t(y)) * uint32_t(g.nz) + uint32_t(z);
-          fcell[0] = __ldg(F + nn);
-          fcell[1] = __ldg(F + size_t(g.stride) + nn);
-          fcell[2] = __ldg(F + 2 * size_t(g.stride) + nn);
-        }
+        if (field && (!MASKED || kind == KIND)) load_force(x, fcell);
       }
 #ifndef OLB_B200_EXACT
       if (!MASKED || kind == KIND) {
-        if ((MASKED && pe) || field) {
-          DynDevice<float> q;
-          if (MASKED && pe) {
-            q.omega = __ldg(&pe->omega);
-            q.omega_minus = __ldg(&pe->omega_minus);
-            q.smago_pre = __ldg(&pe->smago_pre);
-            q.tau_mol = __ldg(&pe->tau_mol);
-            q.force[0] = __ldg(&pe->force[0]);
-            q.force[1] = __ldg(&pe->force[1]);
-            q.force[2] = __ldg(&pe->force[2]);
-            q.force_relax = __ldg(&pe->force_relax);
-          } else {
-            q.omega = bulk.omega;
-            q.omega_minus = bulk.omega_minus;
-            q.smago_pre = bulk.smago_pre;
-            q.tau_mol = bulk.tau_mol;
-            q.force_relax = bulk.force_relax;
-          }
-          if (field) {
-            q.force[0] = fcell[0]; q.force[1] = fcell[1]; q.force[2] = fcell[2];
-          }
-          collide_scaled<L, KIND>(gout, q, r, u2);
-        } else {
-          collide_scaled<L, KIND>(gout, bulk, r, u2);
+        ScaledParams<float> q = scaled_params<KIND>(pe, MASKED && !g.uniform, bulk);
+        if (field) {
+          q.force[0] = fcell[0]; q.force[1] = fcell[1]; q.force[2] = fcell[2];
         }
+        collide_scaled<L, KIND>(gout, q, r, u2);
         counted = true;
         done = true;
       }
@@ -686,7 +772,7 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
           constexpr float inv = 1.f / storage_scale<L>(i);
           gout[i] *= inv;
         });
-        counted = collide_any<L, KIND, MASKED>(gout, kind, pe, bulk, fcell, field, r, u2);
+        counted = collide_any<L, KIND, MASKED>(gout, kind, pe, bulk, fcell, field, g.uniform != 0, r, u2);
         static_for<0, Q>([&](auto i) {
           constexpr float sc = storage_scale<L>(i);
           gout[i] *= sc;
@@ -709,11 +795,9 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
         if (counted) acc.add(double(r), double(u2));
       }
     };
-    // the table entries (nullptr: the bulk entry, the kernel argument)
-    cell(std::integral_constant<bool, false>{}, kind_lo[k],
-         MASKED && id_lo[k] != kBoxCell ? table + id_lo[k] : nullptr);
-    cell(std::integral_constant<bool, true>{}, kind_hi[k],
-         MASKED && id_hi[k] != kBoxCell ? table + id_hi[k] : nullptr);
+    cell(std::integral_constant<bool, false>{}, kind_lo[k], pe_lo);
+    cell(std::integral_constant<bool, true>{}, kind_hi[k], pe_hi);
+    }
     // recomputed after the collision rather than kept live through it
     PairNeighbours nb(g, int(opaque(uint32_t(xp))), int(opaque(uint32_t(y))), int(opaque(uint32_t(z))));
     const uint32_t ps = opaque(pstride);

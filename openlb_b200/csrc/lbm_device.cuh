@@ -938,45 +938,157 @@ OLB_HD constexpr float inv_class_scale(int k)
   return first_of_class<L>(k) < L::q ? 1.f / storage_scale<L>(first_of_class<L>(k)) : 0.f;
 }
 
+// Arithmetic on one cell (V = float) or on the two cells of a packed 16-bit
+// pair at once (V = float2: sm_100's packed FP32 instructions, one instruction
+// for both lanes, each lane rounded as its scalar counterpart).
+OLB_DEV float v_add(float a, float b) { return a + b; }
+OLB_DEV float v_sub(float a, float b) { return a - b; }
+OLB_DEV float v_mul(float a, float b) { return a * b; }
+OLB_DEV float v_fma(float a, float b, float c) { return fmaf(a, b, c); }
+OLB_DEV float v_rcp(float a) { return 1.f / a; }
+OLB_DEV float v_sqrt(float a) { return sqrtf(a); }
+OLB_DEV float2 v_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b as a + (-1) b: the product is exact, so one rounding as in a - b
+OLB_DEV float2 v_sub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+OLB_DEV float2 v_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+OLB_DEV float2 v_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+OLB_DEV float2 v_rcp(float2 a) { return make_float2(1.f / a.x, 1.f / a.y); }
+OLB_DEV float2 v_sqrt(float2 a) { return make_float2(sqrtf(a.x), sqrtf(a.y)); }
+template <class V> OLB_DEV V v_splat(float x);
+template <> OLB_DEV float v_splat<float>(float x) { return x; }
+template <> OLB_DEV float2 v_splat<float2>(float x) { return make_float2(x, x); }
+
+// The collisions on g work on the opposite pairs p = 1..half.  The pair's
+// representative r is the member whose first nonzero velocity component is
+// +1, so every c_r . u starts with a positive term; the pair sum is
+// s_p = g_r + g_opp(r) and the difference d_p = g_r - g_opp(r) (s_i = s_opp, so
+// the pair shares one scale).
 template <class L>
-OLB_DEV void scaled_rho_u(const float (&g)[L::q], float& rho, float& delta, float (&u)[3])
+OLB_HD constexpr int pair_rep(int p)
 {
-  float m[4] = {0.f, 0.f, 0.f, 0.f};
-  float j[3][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
-  static_for<0, L::q>([&](auto i) {
-    constexpr int k = weight_class<L>(i);
-    m[k] += g[i];
-    static_for<0, 3>([&](auto d) {
-      constexpr int cc = L::c(i, d);
-      if constexpr (cc == 1) { j[d][k] += g[i]; }
-      else if constexpr (cc == -1) { j[d][k] -= g[i]; }
+  return L::c(p, 0) != 0 ? (L::c(p, 0) > 0 ? p : L::opp(p))
+       : L::c(p, 1) != 0 ? (L::c(p, 1) > 0 ? p : L::opp(p))
+                         : (L::c(p, 2) > 0 ? p : L::opp(p));
+}
+
+// the first pair of weight class k (in pair order), 0 when the class is empty
+template <class L>
+OLB_HD constexpr int first_pair_of_class(int k)
+{
+  for (int p = 1; p <= L::half; ++p) {
+    if (weight_class<L>(p) == k) return p;
+  }
+  return 0;
+}
+
+// the first pair of weight class k whose velocity has a component along axis
+// a, 0 when there is none
+template <class L>
+OLB_HD constexpr int first_pair_on_axis(int a, int k)
+{
+  for (int p = 1; p <= L::half; ++p) {
+    if (weight_class<L>(p) == k && L::c(pair_rep<L>(p), a) != 0) return p;
+  }
+  return 0;
+}
+
+// the first weight class >= 1 with a pair on axis a (a = -1: any pair)
+template <class L>
+OLB_HD constexpr int first_class_with_pairs(int a)
+{
+  for (int k = 1; k < 4; ++k) {
+    if (a < 0 ? first_pair_of_class<L>(k) != 0 : first_pair_on_axis<L>(a, k) != 0) return k;
+  }
+  return 0;
+}
+
+// c_r . v with a positive first term (r the pair's representative)
+template <class L, int P, class V>
+OLB_DEV V rep_dot(const V (&v)[3])
+{
+  constexpr int r = pair_rep<L>(P);
+  constexpr int c0 = L::c(r, 0), c1 = L::c(r, 1), c2 = L::c(r, 2);
+  V acc;
+  bool first = true;
+  auto term = [&](int c, const V& x) {
+    if (c == 0) return;
+    acc = first ? x : (c > 0 ? v_add(acc, x) : v_sub(acc, x));
+    first = false;
+  };
+  term(c0, v[0]);
+  term(c1, v[1]);
+  term(c2, v[2]);
+  return acc;
+}
+
+// Density from g_0 and the pair sums, velocity from the pair differences: one
+// multiply by 1/s per weight class; a per-axis sum is kept with the sign of
+// its first term folded into that multiplier.
+// live: 1 for a fluid lane, 0 for a bounce-back lane, whose velocity is then
+// its momentum (no division by a density that its stale populations may not
+// give); rinv returns the reciprocal used.
+template <class L, class V>
+OLB_DEV void scaled_moments(const V& g0, const V (&ps)[L::half + 1], const V (&pd)[L::half + 1], const V& live,
+                            V& rho, V& delta, V (&u)[3], V& rinv)
+{
+  V m[4], j[3][4];
+  static_for<1, L::half + 1>([&](auto p) {
+    constexpr int k = weight_class<L>(p.value);
+    constexpr int r = pair_rep<L>(p.value);
+    if constexpr (first_pair_of_class<L>(k) == p.value) {
+      m[k] = ps[p];
+    } else {
+      m[k] = v_add(m[k], ps[p]);
+    }
+    static_for<0, 3>([&](auto a) {
+      constexpr int cc = L::c(r, a);
+      if constexpr (cc != 0) {
+        constexpr int f = first_pair_on_axis<L>(a, k);
+        constexpr int s0 = L::c(pair_rep<L>(f), a);
+        if constexpr (f == p.value) {
+          j[a][k] = pd[p];
+        } else if constexpr (cc == s0) {
+          j[a][k] = v_add(j[a][k], pd[p]);
+        } else {
+          j[a][k] = v_sub(j[a][k], pd[p]);
+        }
+      }
     });
   });
-  delta = 0.f;
-  u[0] = u[1] = u[2] = 0.f;
-  static_for<0, 4>([&](auto k) {
-    constexpr float inv = inv_class_scale<L>(k);
-    if constexpr (inv != 0.f) {
-      delta += m[k] * inv;
-      u[0] += j[0][k] * inv;
-      u[1] += j[1][k] * inv;
-      u[2] += j[2][k] * inv;
+  delta = v_mul(g0, v_splat<V>(inv_class_scale<L>(0)));
+  static_for<1, 4>([&](auto k) {
+    if constexpr (first_pair_of_class<L>(k) != 0) {
+      delta = v_fma(m[k], v_splat<V>(inv_class_scale<L>(k)), delta);
     }
   });
-  rho = delta + 1.f;
-  const float r = 1.f / rho;
-  u[0] *= r; u[1] *= r; u[2] *= r;
+  static_for<0, 3>([&](auto a) {
+    static_for<1, 4>([&](auto k) {
+      constexpr int f = first_pair_on_axis<L>(a, k);
+      if constexpr (f != 0) {
+        constexpr float inv = float(L::c(pair_rep<L>(f), a)) * inv_class_scale<L>(k);
+        if constexpr (first_class_with_pairs<L>(a) == k) {
+          u[a] = v_mul(j[a][k], v_splat<V>(inv));
+        } else {
+          u[a] = v_fma(j[a][k], v_splat<V>(inv), u[a]);
+        }
+      }
+    });
+  });
+  rho = v_add(delta, v_splat<V>(1.f));
+  rinv = v_rcp(v_fma(rho, live, v_sub(v_splat<V>(1.f), live)));
+  u[0] = v_mul(u[0], rinv);
+  u[1] = v_mul(u[1], rinv);
+  u[2] = v_mul(u[2], rinv);
 }
 
 // BGK / TRT relaxation on g in pair form, with the Guo force term folded in.
-// For a pair (i, opp) with sum s = g_i + g_opp and difference d = g_i - g_opp,
-//   TRT:  g_i' = S + D,  g_opp' = S - D,
-//         S = (1 - omega)/2 s + A,  D = (1 - omega_minus)/2 d + B
-//   BGK:  g_i' = (1 - omega) g_i + A + B,  g_opp' = (1 - omega) g_opp + A - B
-// with the equilibrium parts of A and B (per weight class k = s_i t_i):
+// For a pair with representative r, sum s and difference d,
+//   g_r' = S + D,  g_opp(r)' = S - D,
+//   S = keep s + A,  D = keep' d + B,  keep = (1 - omega)/2,  keep' = (1 - omega')/2
+// (omega' = omega_minus for TRT, omega for BGK) with the equilibrium parts of
+// A and B (per weight class k = s_i t_i):
 //   A = omega k (delta + rho (9/2 (c.u)^2 - 3/2 |u|^2)),  B = 3 omega' k rho (c.u)
-// (omega' = omega_minus for TRT, omega for BGK) and the Guo term of
-// lbm::addExternalForce (src/dynamics/lbm.h:544-566),
+// and the Guo term of lbm::addExternalForce (src/dynamics/lbm.h:544-566),
 //   t_i (3 (c_i - u).F + 9 (c_i.u)(c_i.F)) force_relax rho,
 // which over a pair is Fa +- Fb with Fa = k fr (9 (c.u)(c.F) - 3 u.F) and
 // Fb = 3 k fr (c.F), fr = force_relax rho: A += Fa, B += Fb.  Everything that
@@ -985,114 +1097,140 @@ OLB_DEV void scaled_rho_u(const float (&g)[L::q], float& rho, float& delta, floa
 // with entries of +-1 and about a dozen FP32 operations.  The same collision
 // as relaxing and then adding the force (the rounding differs far below the
 // 16-bit storage's own).
-template <class L, bool TRT, bool FORCED>
-OLB_DEV void relax_scaled(float (&g)[L::q], float rho, float delta, const float (&u)[3], float usqr,
-                          float omega, float omega_minus, float force_relax, const float (&gf)[3])
+template <class L, bool FORCED, class V>
+OLB_DEV void relax_scaled(V (&g)[L::q], const V (&ps)[L::half + 1], const V (&pd)[L::half + 1], const V& rho,
+                          const V& delta, const V (&u)[3], const V& usqr, const V& omega, const V& omega_b,
+                          const V& keep, const V& keep_minus, const V& force_relax, const V (&gf)[3])
 {
-  const float base = delta - 1.5f * rho * usqr;  // delta + rho e0
-  const float rho45 = 4.5f * rho;
-  const float rho_odd = (TRT ? omega_minus : omega) * rho;
-  float fr = 0.f, uf3 = 0.f;
+  const V base = v_fma(v_mul(v_splat<V>(-1.5f), rho), usqr, delta);  // delta + rho e0
+  const V rho45 = v_mul(v_splat<V>(4.5f), rho);
+  const V rho_odd = v_mul(omega_b, rho);
+  V fr = v_splat<V>(0.f), uf3 = v_splat<V>(0.f);
   if constexpr (FORCED) {
-    fr = force_relax * rho;
-    uf3 = 3.f * (u[0] * gf[0] + u[1] * gf[1] + u[2] * gf[2]);
+    fr = v_mul(force_relax, rho);
+    uf3 = v_mul(v_splat<V>(3.f), v_fma(u[2], gf[2], v_fma(u[1], gf[1], v_mul(u[0], gf[0]))));
   }
   {
     constexpr float T = storage_scale<L>(0) * weight<L, float>(0);
-    float eq = (omega * T) * base;
-    if constexpr (FORCED) eq -= (T * fr) * uf3;
-    g[0] = fmaf(1.f - omega, g[0], eq);
+    V eq = v_mul(v_mul(omega, v_splat<V>(T)), base);
+    if constexpr (FORCED) eq = v_fma(v_mul(v_splat<V>(-T), fr), uf3, eq);
+    g[0] = v_fma(v_sub(v_splat<V>(1.f), omega), g[0], eq);
   }
-  const float keep = TRT ? 0.5f * (1.f - omega) : 1.f - omega;
-  const float keep_minus = 0.5f * (1.f - omega_minus);
-  static_for<1, L::half + 1>([&](auto i) {
-    constexpr int o = L::opp(i);
-    constexpr float T = storage_scale<L>(i) * weight<L, float>(i);
+  static_for<1, L::half + 1>([&](auto p) {
+    constexpr int r = pair_rep<L>(p.value);
+    constexpr int o = L::opp(r);
+    constexpr float T = storage_scale<L>(r) * weight<L, float>(r);
     constexpr float K = 3.f * T;
-    const float wt = omega * T;
-    const float cu = c_dot<L, i.value>(u);
-    float a0 = wt * base;
-    float A, B;
+    const V wt = v_mul(omega, v_splat<V>(T));
+    const V cu = rep_dot<L, p.value>(u);
+    V a0 = v_mul(wt, base);
+    V A, B;
     if constexpr (FORCED) {
-      const float kf = T * fr;
-      a0 = fmaf(-kf, uf3, a0);
-      const float cf = c_dot<L, i.value>(gf);
-      A = fmaf(wt * rho45, cu * cu, fmaf(9.f * kf, cu * cf, a0));
-      B = fmaf(K * rho_odd, cu, (3.f * kf) * cf);
+      const V kf = v_mul(v_splat<V>(T), fr);
+      a0 = v_fma(v_mul(v_splat<V>(-1.f), kf), uf3, a0);
+      const V cf = rep_dot<L, p.value>(gf);
+      A = v_fma(v_mul(wt, rho45), v_mul(cu, cu), v_fma(v_mul(v_splat<V>(9.f), kf), v_mul(cu, cf), a0));
+      B = v_fma(v_mul(v_splat<V>(K), rho_odd), cu, v_mul(v_mul(v_splat<V>(3.f), kf), cf));
     } else {
-      A = fmaf(wt * rho45, cu * cu, a0);
-      B = (K * rho_odd) * cu;
+      A = v_fma(v_mul(wt, rho45), v_mul(cu, cu), a0);
+      B = v_mul(v_mul(v_splat<V>(K), rho_odd), cu);
     }
-    if constexpr (TRT) {
-      const float S = fmaf(keep, g[i] + g[o], A);
-      const float D = fmaf(keep_minus, g[i] - g[o], B);
-      g[i] = S + D;
-      g[o] = S - D;
-    } else {
-      g[i] = fmaf(keep, g[i], A + B);
-      g[o] = fmaf(keep, g[o], A - B);
-    }
+    const V S = v_fma(keep, ps[p], A);
+    const V D = v_fma(keep_minus, pd[p], B);
+    g[r] = v_add(S, D);
+    g[o] = v_sub(S, D);
   });
 }
 
 // Smagorinsky effective omega from the scaled populations: Pi_ab per weight
-// class from pair sums (g_i + g_opp), one multiply by 1/s per class.
-template <class L>
-OLB_DEV float smagorinsky_omega_scaled(const float (&g)[L::q], float rho, float delta, const float (&u)[3],
-                                       float smago_pre, float tau_mol)
+// class from the pair sums, one multiply by 1/s per class.
+template <class L, class V>
+OLB_DEV V smagorinsky_omega_scaled(const V (&ps)[L::half + 1], const V& rho, const V& rinv, const V& delta,
+                                   const V (&u)[3], const V& smago_pre, const V& tau_mol)
 {
-  float pik[6][4] = {};
-  static_for<1, L::half + 1>([&](auto i) {
-    constexpr int k = weight_class<L>(i);
-    const float P = g[i] + g[L::opp(i)];
+  V pik[6][4];
+  static_for<0, 6>([&](auto m) { static_for<0, 4>([&](auto k) { pik[m][k] = v_splat<V>(-0.f); }); });
+  static_for<1, L::half + 1>([&](auto p) {
+    constexpr int k = weight_class<L>(p.value);
+    constexpr int r = pair_rep<L>(p.value);
     static_for<0, 3>([&](auto a) {
       static_for<a.value, 3>([&](auto b) {
         constexpr int m = a.value * 3 - (a.value * (a.value - 1)) / 2 + (b.value - a.value);
-        constexpr int cc = L::c(i, a) * L::c(i, b);
-        if constexpr (cc == 1) { pik[m][k] += P; }
-        else if constexpr (cc == -1) { pik[m][k] -= P; }
+        constexpr int cc = L::c(r, a) * L::c(r, b);
+        if constexpr (cc == 1) { pik[m][k] = v_add(pik[m][k], ps[p]); }
+        else if constexpr (cc == -1) { pik[m][k] = v_sub(pik[m][k], ps[p]); }
       });
     });
   });
-  float pi[6];
+  V pi[6];
   static_for<0, 3>([&](auto a) {
     static_for<a.value, 3>([&](auto b) {
       constexpr int m = a.value * 3 - (a.value * (a.value - 1)) / 2 + (b.value - a.value);
-      float s = 0.f;
+      V s = v_splat<V>(-0.f);
       static_for<1, 4>([&](auto k) {
         constexpr float inv = inv_class_scale<L>(k);
-        if constexpr (inv != 0.f) { s += pik[m][k] * inv; }
+        if constexpr (inv != 0.f) { s = v_fma(pik[m][k], v_splat<V>(inv), s); }
       });
-      s -= rho * u[a] * u[b];
-      if constexpr (a.value == b.value) { s -= (1.f / 3.f) * delta; }
+      s = v_sub(s, v_mul(v_mul(rho, u[a]), u[b]));
+      if constexpr (a.value == b.value) { s = v_sub(s, v_mul(v_splat<V>(1.f / 3.f), delta)); }
       pi[m] = s;
     });
   });
-  const float n2 = pi[0] * pi[0] + pi[3] * pi[3] + pi[5] * pi[5] + 2.f * (pi[1] * pi[1] + pi[2] * pi[2] + pi[4] * pi[4]);
-  const float tau_turb = 0.5f * (sqrtf(tau_mol * tau_mol + smago_pre / rho * sqrtf(n2)) - tau_mol);
-  return 1.f / (tau_mol + tau_turb);
+  const V diag = v_fma(pi[5], pi[5], v_fma(pi[3], pi[3], v_mul(pi[0], pi[0])));
+  const V off = v_fma(pi[4], pi[4], v_fma(pi[2], pi[2], v_mul(pi[1], pi[1])));
+  const V n2 = v_fma(v_splat<V>(2.f), off, diag);
+  const V inner = v_fma(v_mul(smago_pre, rinv), v_sqrt(n2), v_mul(tau_mol, tau_mol));
+  const V tau_turb = v_mul(v_splat<V>(0.5f), v_sub(v_sqrt(inner), tau_mol));
+  return v_rcp(v_add(tau_mol, tau_turb));
 }
 
+// Collision constants of the fluid dynamics for the scaled collisions, one
+// value per lane: omega (weight of the symmetric equilibrium part), omega_b
+// (of the antisymmetric part: omega_minus for TRT, omega for BGK), keep =
+// (1 - omega)/2, keep_minus = (1 - omega_b)/2.  A bounce-back lane has omega =
+// omega_b = force_relax = 0, keep = 1/2, keep_minus = -1/2 and live = 0: the
+// same arithmetic then gives S = s/2, D = -d/2, so g_r' = g_opp, g_opp' = g_r
+// and g_0' = g_0 — full-way bounce-back (collision::Revert), exact once
+// rounded to the 16-bit storage the populations came from.
+template <class V>
+struct ScaledParams {
+  V omega, omega_b, keep, keep_minus, force_relax, smago_pre, tau_mol, live;
+  V force[3];
+};
+
 // Any fluid collision on the scaled 16-bit representation (see above).
-template <class L, int KIND>
-OLB_DEV void collide_scaled(float (&g)[L::q], const DynDevice<float>& p, float& st_rho, float& st_usqr)
+template <class L, int KIND, class V>
+OLB_DEV void collide_scaled(V (&g)[L::q], const ScaledParams<V>& p, V& st_rho, V& st_usqr)
 {
-  float rho, delta, u[3];
-  scaled_rho_u<L>(g, rho, delta, u);
+  V ps[L::half + 1], pd[L::half + 1];
+  static_for<1, L::half + 1>([&](auto q) {
+    constexpr int r = pair_rep<L>(q.value);
+    constexpr int o = L::opp(r);
+    ps[q] = v_add(g[r], g[o]);
+    pd[q] = v_sub(g[r], g[o]);
+  });
+  V rho, delta, u[3], rinv;
+  scaled_moments<L>(g[0], ps, pd, p.live, rho, delta, u, rinv);
   constexpr bool forced = KIND == K_FORCED_BGK || KIND == K_FORCED_TRT;
-  float gf[3] = {0.f, 0.f, 0.f};
+  V gf[3] = {v_splat<V>(0.f), v_splat<V>(0.f), v_splat<V>(0.f)};
   if constexpr (forced) {
     gf[0] = p.force[0]; gf[1] = p.force[1]; gf[2] = p.force[2];
-    u[0] += gf[0] * 0.5f; u[1] += gf[1] * 0.5f; u[2] += gf[2] * 0.5f;
+    const V half = v_splat<V>(0.5f);
+    u[0] = v_fma(gf[0], half, u[0]);
+    u[1] = v_fma(gf[1], half, u[1]);
+    u[2] = v_fma(gf[2], half, u[2]);
   }
-  const float usqr = norm_sqr(u);
-  if constexpr (KIND == K_TRT || KIND == K_FORCED_TRT) {
-    relax_scaled<L, true, forced>(g, rho, delta, u, usqr, p.omega, p.omega_minus, p.force_relax, gf);
-  } else if constexpr (KIND == K_SMAGORINSKY) {
-    const float w = smagorinsky_omega_scaled<L>(g, rho, delta, u, p.smago_pre, p.tau_mol);
-    relax_scaled<L, false, false>(g, rho, delta, u, usqr, w, w, 0.f, gf);
+  const V usqr = v_fma(u[2], u[2], v_fma(u[1], u[1], v_mul(u[0], u[0])));
+  if constexpr (KIND == K_SMAGORINSKY) {
+    // the cell's effective omega; a bounce-back lane (live = 0) gets 0 and
+    // keep_minus = -1/2
+    const V w = v_mul(smagorinsky_omega_scaled<L>(ps, rho, rinv, delta, u, p.smago_pre, p.tau_mol), p.live);
+    const V keep = v_mul(v_splat<V>(0.5f), v_sub(v_splat<V>(1.f), w));
+    const V keep_minus = v_fma(p.live, v_add(keep, v_splat<V>(0.5f)), v_splat<V>(-0.5f));
+    relax_scaled<L, false>(g, ps, pd, rho, delta, u, usqr, w, w, keep, keep_minus, v_splat<V>(0.f), gf);
   } else {
-    relax_scaled<L, false, forced>(g, rho, delta, u, usqr, p.omega, p.omega, p.force_relax, gf);
+    relax_scaled<L, forced>(g, ps, pd, rho, delta, u, usqr, p.omega, p.omega_b, p.keep, p.keep_minus,
+                            p.force_relax, gf);
   }
   st_rho = rho;
   st_usqr = usqr;

@@ -866,6 +866,20 @@ olb_b200_status olb_b200_set_dynamics(olb_b200_lattice* L, const uint8_t* ids,
     std::memcpy(L->bulk, host.data() + only * esz, esz);
   }
   compute_bulk_box(L, L->masked ? ids : nullptr, bulk);
+  // the masked kernels take the bulk entry's constants for every cell of its
+  // kind when no other entry of that kind differs from it
+  L->g.uniform = 0;
+  if (L->masked && bulk >= 0) {
+    bool same = true;
+    const olb_b200_dyn_params& b = table[bulk];
+    for (int k = 0; k < n_entries && same; ++k) {
+      const olb_b200_dyn_params& e = table[k];
+      if (e.kind != b.kind) continue;
+      same = e.omega == b.omega && e.magic == b.magic && e.smagorinsky == b.smagorinsky &&
+             e.force[0] == b.force[0] && e.force[1] == b.force[1] && e.force[2] == b.force[2];
+    }
+    L->g.uniform = same ? 1 : 0;
+  }
   L->n_entries = n_entries;
   // a change of kernel class invalidates an earlier tuning
   if (!L->tuned || was_masked != L->masked) {
