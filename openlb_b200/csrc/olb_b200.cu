@@ -319,7 +319,9 @@ void default_shape(const olb_b200_lattice* L, int& bz, int& by)
 int default_variant(const olb_b200_lattice* L)
 {
   const int storage = L->desc.storage;
-  if (storage == OLB_B200_STORAGE_F16 || storage == OLB_B200_STORAGE_BF16) return 1;  // {1,4}
+  // 16-bit: D3Q19's two-lane collision fits the 64-register cap of {1,4};
+  // D3Q27's needs the 80 registers of {1,3}
+  if (storage == OLB_B200_STORAGE_F16 || storage == OLB_B200_STORAGE_BF16) return L->q == 27 ? 0 : 1;
   if (L->masked) return storage == OLB_B200_STORAGE_F64 ? 0 : 1;                  // {1,3} / {1,4}
   if (storage == OLB_B200_STORAGE_F64) return 2;                                     // {2,2}
   return 3;                                                                          // {2,3}
