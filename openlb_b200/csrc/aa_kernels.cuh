@@ -461,13 +461,19 @@ template <> struct Pair<__nv_bfloat16> {
   OLB_DEV static T from_float2(float2 v) { return __float22bfloat162_rn(v); }
 };
 
+// what a lane of the two-lane collision does: collide with the lattice's fluid
+// kind, bounce back (full-way, collision::Revert), or pass its populations
+// through unchanged (NoDynamics, and boundary cells, whose collision ran ahead
+// of the step kernel)
+enum LaneMode { kLaneFluid = 0, kLaneWall = 1, kLanePass = 2 };
+
 // the fluid collision constants of a cell for the scaled collisions (KIND the
 // lattice's fluid kind): its table entry's when `own` and it has one, else the
-// bulk entry's (kernel argument); `wall`: the constants that make the same
-// arithmetic a full-way bounce-back (see ScaledParams)
+// bulk entry's (kernel argument); a wall or pass lane gets the constants that
+// make the same arithmetic a swap or the identity (see ScaledParams)
 template <int KIND>
 OLB_DEV ScaledParams<float> scaled_params(const DynDevice<float>* pe, bool own, const DynDevice<float>& bulk,
-                                          bool wall = false)
+                                          int lane = kLaneFluid)
 {
   ScaledParams<float> q;
   if (own && pe) {
@@ -493,11 +499,11 @@ OLB_DEV ScaledParams<float> scaled_params(const DynDevice<float>* pe, bool own, 
   q.keep = 0.5f * (1.f - q.omega);
   q.keep_minus = 0.5f * (1.f - q.omega_b);
   q.live = 1.f;
-  if (wall) {
+  if (lane != kLaneFluid) {
     q.omega = q.omega_b = q.force_relax = 0.f;
     q.force[0] = q.force[1] = q.force[2] = 0.f;
     q.keep = 0.5f;
-    q.keep_minus = -0.5f;
+    q.keep_minus = lane == kLaneWall ? -0.5f : 0.5f;
     q.live = 0.f;
   }
   return q;
@@ -697,28 +703,33 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
       fc[2] = __ldg(F + 2 * size_t(g.stride) + nn);
     };
 #ifndef OLB_B200_EXACT
-    // both cells collide with the lattice's fluid kind, or one of them is a
-    // full-way bounce-back wall (a pair of two walls stores nothing)
+    // both cells go through the two-lane collision unless one is a moving wall
+    // (a pair of two bounce-back walls stores nothing)
     bool both = true;
-    bool wall_lo = false, wall_hi = false;
+    int lane_lo = kLaneFluid, lane_hi = kLaneFluid;
     if constexpr (MASKED) {
-      wall_lo = kind_lo[k] == K_BOUNCE_BACK;
-      wall_hi = kind_hi[k] == K_BOUNCE_BACK;
-      both = (kind_lo[k] == KIND || wall_lo) && (kind_hi[k] == KIND || wall_hi);
+      auto mode = [](int kind) {
+        return kind == KIND ? kLaneFluid : (kind == K_BOUNCE_BACK ? kLaneWall : kLanePass);
+      };
+      lane_lo = mode(kind_lo[k]);
+      lane_hi = mode(kind_hi[k]);
+      // a moving wall adds its momentum terms: one cell after the other
+      both = kind_lo[k] != K_BOUNCE_BACK_VELOCITY && kind_hi[k] != K_BOUNCE_BACK_VELOCITY;
     }
     if (both) {
       // Both cells at once, in the scaled representation g_i = s_i (f_i - w_i)
       // of the storage: lane x the low cell, lane y the high one, straight
-      // from and back to the packed pairs (packed FP32 arithmetic); a wall
-      // lane takes the constants that make the collision a bounce-back.
+      // from and back to the packed pairs (packed FP32 arithmetic); a wall or
+      // pass lane takes the constants that make the collision a bounce-back or
+      // the identity.
       float2 g2[Q];
       static_for<0, Q>([&](auto i) { g2[i] = P::to_float2(raw[k][i]); });
-      ScaledParams<float> lo = scaled_params<KIND>(pe_lo, MASKED && !g.uniform, bulk, wall_lo);
-      ScaledParams<float> hi = scaled_params<KIND>(pe_hi, MASKED && !g.uniform, bulk, wall_hi);
+      ScaledParams<float> lo = scaled_params<KIND>(pe_lo, MASKED && !g.uniform, bulk, lane_lo);
+      ScaledParams<float> hi = scaled_params<KIND>(pe_hi, MASKED && !g.uniform, bulk, lane_hi);
       if constexpr (kForced) {
         if (field) {
-          if (!wall_lo) load_force(xp, lo.force);
-          if (!wall_hi) load_force(xp + (g.nx >> 1), hi.force);
+          if (lane_lo == kLaneFluid) load_force(xp, lo.force);
+          if (lane_hi == kLaneFluid) load_force(xp + (g.nx >> 1), hi.force);
         }
       }
       const ScaledParams<float2> q2 = zip_params(lo, hi);
@@ -726,8 +737,8 @@ OLB_DEV void paired_tile(S* __restrict__ pops_scalar, const Geometry& g, const D
       collide_scaled<L, KIND>(g2, q2, r2, u22);
       static_for<0, Q>([&](auto i) { raw[k][i] = P::from_float2(g2[i]); });
       if constexpr (STATS) {
-        if (!wall_lo) acc.add(double(r2.x), double(u22.x));
-        if (!wall_hi) acc.add(double(r2.y), double(u22.y));
+        if (lane_lo == kLaneFluid) acc.add(double(r2.x), double(u22.x));
+        if (lane_hi == kLaneFluid) acc.add(double(r2.y), double(u22.y));
       }
     } else
 #endif

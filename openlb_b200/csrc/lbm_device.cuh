@@ -954,6 +954,12 @@ OLB_DEV float2 v_mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
 OLB_DEV float2 v_fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 OLB_DEV float2 v_rcp(float2 a) { return make_float2(1.f / a.x, 1.f / a.y); }
 OLB_DEV float2 v_sqrt(float2 a) { return make_float2(sqrtf(a.x), sqrtf(a.y)); }
+// live != 0 ? a : b, per lane
+OLB_DEV float v_select(float live, float a, float b) { return live != 0.f ? a : b; }
+OLB_DEV float2 v_select(float2 live, float2 a, float2 b)
+{
+  return make_float2(live.x != 0.f ? a.x : b.x, live.y != 0.f ? a.y : b.y);
+}
 template <class V> OLB_DEV V v_splat(float x);
 template <> OLB_DEV float v_splat<float>(float x) { return x; }
 template <> OLB_DEV float2 v_splat<float2>(float x) { return make_float2(x, x); }
@@ -1190,8 +1196,10 @@ OLB_DEV V smagorinsky_omega_scaled(const V (&ps)[L::half + 1], const V& rho, con
 // (1 - omega)/2, keep_minus = (1 - omega_b)/2.  A bounce-back lane has omega =
 // omega_b = force_relax = 0, keep = 1/2, keep_minus = -1/2 and live = 0: the
 // same arithmetic then gives S = s/2, D = -d/2, so g_r' = g_opp, g_opp' = g_r
-// and g_0' = g_0 — full-way bounce-back (collision::Revert), exact once
-// rounded to the 16-bit storage the populations came from.
+// and g_0' = g_0 — full-way bounce-back (collision::Revert) up to one FP32
+// rounding of the pair's sum and difference (2^-24 of the pair's larger
+// member, far below the 16-bit storage's own rounding).  A pass lane
+// (keep_minus = +1/2) gives g' = g the same way.
 template <class V>
 struct ScaledParams {
   V omega, omega_b, keep, keep_minus, force_relax, smago_pre, tau_mol, live;
@@ -1222,11 +1230,11 @@ OLB_DEV void collide_scaled(V (&g)[L::q], const ScaledParams<V>& p, V& st_rho, V
   }
   const V usqr = v_fma(u[2], u[2], v_fma(u[1], u[1], v_mul(u[0], u[0])));
   if constexpr (KIND == K_SMAGORINSKY) {
-    // the cell's effective omega; a bounce-back lane (live = 0) gets 0 and
-    // keep_minus = -1/2
+    // the cell's effective omega; a wall or pass lane (live = 0) gets 0 and
+    // its own keep_minus
     const V w = v_mul(smagorinsky_omega_scaled<L>(ps, rho, rinv, delta, u, p.smago_pre, p.tau_mol), p.live);
     const V keep = v_mul(v_splat<V>(0.5f), v_sub(v_splat<V>(1.f), w));
-    const V keep_minus = v_fma(p.live, v_add(keep, v_splat<V>(0.5f)), v_splat<V>(-0.5f));
+    const V keep_minus = v_select(p.live, keep, p.keep_minus);
     relax_scaled<L, false>(g, ps, pd, rho, delta, u, usqr, w, w, keep, keep_minus, v_splat<V>(0.f), gf);
   } else {
     relax_scaled<L, forced>(g, ps, pd, rho, delta, u, usqr, p.omega, p.omega_b, p.keep, p.keep_minus,
