@@ -367,8 +367,10 @@ size_t step_blocks(const olb_b200_lattice* L)
 // entry, so the step kernel loads no dynamics id for them.  The box starts as
 // the whole lattice and loses any face layer that holds another entry until
 // no face does (for a lattice with walls on its faces, such as the lid-driven
-// cavity, that is the interior); if the box's interior still holds another
-// entry (obstacles inside), no box is used.
+// cavity, that is the interior).  If the box's interior still holds other
+// entries (an obstacle inside, such as a cylinder in a channel), the box
+// becomes the largest of the six slabs of it beside the obstacles' bounding
+// box that holds the bulk entry only, if any.
 void compute_bulk_box(olb_b200_lattice* L, const uint8_t* ids, int bulk_entry)
 {
   Geometry& g = L->g;
@@ -396,10 +398,37 @@ void compute_bulk_box(olb_b200_lattice* L, const uint8_t* ids, int bulk_entry)
     }
     if (!(lo[0] < hi[0] && lo[1] < hi[1] && lo[2] < hi[2])) return;
   }
+  // the bounding box of the other entries inside the box
+  int olo[3] = {hi[0], hi[1], hi[2]}, ohi[3] = {lo[0] - 1, lo[1] - 1, lo[2] - 1};
   for (int x = lo[0]; x < hi[0]; ++x)
     for (int y = lo[1]; y < hi[1]; ++y)
       for (int z = lo[2]; z < hi[2]; ++z)
-        if (id_at(x, y, z) != bulk_entry) return;
+        if (id_at(x, y, z) != bulk_entry) {
+          const int p[3] = {x, y, z};
+          for (int d = 0; d < 3; ++d) {
+            olo[d] = std::min(olo[d], p[d]);
+            ohi[d] = std::max(ohi[d], p[d]);
+          }
+        }
+  if (ohi[0] >= lo[0]) {
+    // six slabs beside the obstacles: below olo[d] or above ohi[d] along axis d
+    size_t best = 0;
+    int blo[3] = {0, 0, 0}, bhi[3] = {0, 0, 0};
+    for (int d = 0; d < 3; ++d) {
+      for (int side = 0; side < 2; ++side) {
+        int a[3] = {lo[0], lo[1], lo[2]}, b[3] = {hi[0], hi[1], hi[2]};
+        if (side == 0) b[d] = olo[d]; else a[d] = ohi[d] + 1;
+        if (!(a[d] < b[d])) continue;
+        const size_t vol = size_t(b[0] - a[0]) * size_t(b[1] - a[1]) * size_t(b[2] - a[2]);
+        if (vol > best) {
+          best = vol;
+          for (int e = 0; e < 3; ++e) { blo[e] = a[e]; bhi[e] = b[e]; }
+        }
+      }
+    }
+    if (best == 0) return;
+    for (int d = 0; d < 3; ++d) { lo[d] = blo[d]; hi[d] = bhi[d]; }
+  }
   for (int d = 0; d < 3; ++d) { g.bulk_lo[d] = lo[d]; g.bulk_hi[d] = hi[d]; }
 }
 
